@@ -1,0 +1,179 @@
+/* liblbmb200 - B200-native D3Q19 TRT lattice-Boltzmann solver, flat C ABI.
+ *
+ * Plain pointers and sizes only; every function returns an int status
+ * (LBM_OK = 0, negative on error; lbm_last_error() gives the message) unless
+ * stated otherwise. All solver state lives in device memory; the host arrays
+ * below are read or written only by the calls that take them.
+ *
+ * Array conventions
+ *   flags  int[nx*ny*nz] in LBM-Bench's latticeIndex order, x fastest
+ *          (src/lbm.h:108-111): 0 = obstacle (LAT_CELL_OBSTACLE), any other
+ *          value = fluid (LAT_CELL_FLUID/INLET/OUTLET, src/lbm.h:47-52).
+ *   f      double[19*nx*ny*nz], f[((d*nx + x)*ny + y)*nz + z]: the
+ *          population of direction d that cell (x,y,z) collides next, i.e.
+ *          what the reference's kd->GetNode returns (src/lbm.c:193-294);
+ *          z is the unit-stride axis as in the reference's indexSoA
+ *          (src/lbm.h:113-116), without the ghost layer. Direction order
+ *          N,S,E,W,NE,SE,NW,SW,T,TN,TE,TW,TS,B,BS,BN,BW,BE,C (src/lbm.h:20-38).
+ *   cell arrays (porosity, moments, gradients): [nx*ny*nz], same cell order
+ *          as one plane of f.
+ *
+ * Threading: a solver is driven by one host thread at a time; its GPU work
+ * runs in order on the solver's own CUDA stream.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_OK 0
+#define LBM_ERR_ARG (-1)       /* invalid argument or unsupported size */
+#define LBM_ERR_CUDA (-2)      /* a CUDA runtime call failed */
+#define LBM_ERR_ALLOC (-3)     /* device or pinned-host allocation failed */
+#define LBM_ERR_NONFINITE (-4) /* the state holds NaN or Inf */
+#define LBM_ERR_STATE (-5)     /* call not valid in the solver's current state */
+#define LBM_ERR_NODEV (-6)     /* no CUDA device (the product has no CPU path) */
+
+/* Propagation patterns, numbered as the reference's PROP_* (src/lbm.h:148). */
+#define LBM_PUSH 0
+#define LBM_PULL 1
+#define LBM_AA 2
+
+/* Storage/arithmetic precision. F64: FP64 populations and arithmetic,
+ * bit-identical to the reference. F32: FP32 arithmetic on shifted
+ * populations f_d - w_d stored as FP32. F16: FP32 arithmetic, shifted
+ * populations stored as FP16 scaled by a power of two. */
+#define LBM_F64 0
+#define LBM_F32 1
+#define LBM_F16 2
+
+typedef struct lbm_solver lbm_solver;
+
+/* Creates a solver on the current CUDA device for an nx*ny*nz box with the
+ * given flags and periodicity. The state starts at zero (as the reference's
+ * Init leaves it, src/lbm.c:452-463). Replaces the reference's
+ * kernelInitInternal (src/lbm.c:400-599) for the pull/push/AA SoA kernels:
+ * instead of bounce-back index lists it builds one 32-bit link mask per
+ * cell on the device. */
+int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *flags, int periodic_x,
+    int periodic_y, int periodic_z, int pattern, int precision);
+
+/* Frees everything the solver owns (src/lbm.c:660-670). NULL is a no-op. */
+int lbm_destroy(lbm_solver *s);
+
+/* Relaxation rate omega (src/main.c:46, -o), TRT magic parameter Lambda
+ * (hard-coded 1/12 at src/kernel_pull_soa.c:20), body force F in x
+ * (src/main.c:47, -f) and whether it is applied after every step (the
+ * reference applies it only in -DVERIFICATION builds,
+ * src/kernel_pull_soa.c:206-209). Defaults: 1.0, 1/12, 1e-5, 0. */
+int lbm_set_params(lbm_solver *s, double omega, double lambda, double xforce, int force_on);
+
+/* FP16 storage scale (power of two, default 16384). F16 solvers only;
+ * only valid before the first lbm_set_state. */
+int lbm_set_fp16_scale(lbm_solver *s, double scale);
+
+/* Per-cell porosity phi in [0,1] (float[nx*ny*nz]) and Brinkman scale alpha:
+ * every fluid cell's collision adds the resistance force
+ * F_b = -alpha (1 - phi) j (j = momentum). alpha = 0 switches it off.
+ * No counterpart in the reference. */
+int lbm_set_porosity(lbm_solver *s, const float *porosity, double alpha);
+
+/* Uploads / downloads the state (array f above). Obstacle entries are
+ * ignored on upload and written as 0 on download. The solver keeps the
+ * state in its pattern's own orientation (like the reference's
+ * Get/SetNode, src/lbm.c:193-294) and converts on the way. */
+int lbm_set_state(lbm_solver *s, const double *f);
+int lbm_get_state(lbm_solver *s, double *f);
+
+/* Enqueues `steps` time steps on the solver's stream (asynchronous).
+ * Replaces the time loop of kd->Kernel (src/kernel_pull_soa.c:44-214,
+ * src/kernel_push_soa.c:44-214, src/kernel_aa_soa.c:36-286); an AA solver
+ * runs single steps, so odd counts are allowed. */
+int lbm_run(lbm_solver *s, int steps);
+int lbm_synchronize(lbm_solver *s);
+
+/* Runs `steps` steps between two CUDA events on the solver's stream, waits,
+ * and returns the elapsed device time in milliseconds. */
+int lbm_run_timed(lbm_solver *s, int steps, double *ms);
+
+/* Runs `steps` steps with an event pair around every launch and returns, per
+ * kernel kind (0 pull, 1 push, 2 AA even, 3 AA odd), the summed device time
+ * (ms_sum[4]) and the launch count (count[4]); *region_ms (may be NULL) gets
+ * the device time from the first launch's start to the last one's end. */
+int lbm_time_launches(lbm_solver *s, int steps, double *ms_sum, int *count, double *region_ms);
+
+/* Page-locks (pins) / releases a caller-owned host buffer so that the state
+ * transfers of lbm_set_state / lbm_get_state run as DMA at full PCIe speed. */
+int lbm_pin_host(void *ptr, size_t bytes);
+int lbm_unpin_host(void *ptr);
+
+/* Per-cell density and momentum (the reference's ux is the momentum,
+ * src/kernel_pull_soa.c:118-126) into host arrays of nx*ny*nz doubles;
+ * obstacle cells get 0. Any pointer may be NULL. */
+int lbm_moments(lbm_solver *s, double *rho, double *ux, double *uy, double *uz);
+
+/* FP64 totals over fluid cells: out[0] = mass, out[1..3] = momentum, with
+ * a fixed-order (deterministic) reduction. *nonfinite (may be NULL) gets
+ * the number of fluid cells holding a NaN/Inf population; if it is
+ * non-zero the call returns LBM_ERR_NONFINITE after filling out.
+ * kernelDensity (src/lbm.c:928-947) is out[0] / lbm_fluid_cells(). */
+int lbm_mass_momentum(lbm_solver *s, double out[4], long long *nonfinite);
+
+/* Difference of two solvers over the same geometry (the first is compared
+ * against the second, e.g. an FP16 run against an FP64 run):
+ * out[0] = sum |u_a - u_b|^2, out[1] = sum |u_b|^2,
+ * out[2] = sum (rho_a - rho_b)^2, out[3] = sum rho_b^2,
+ * out[4] = max |u_a - u_b|,     out[5] = max |u_b|  (u = momentum vector),
+ * all over fluid cells, in FP64 on the device. */
+int lbm_compare(lbm_solver *a, lbm_solver *b, double out[6]);
+
+/* Objective J = mean over the fluid cells of the plane x = nx-1 of the x
+ * momentum. No counterpart in the reference. */
+int lbm_objective(lbm_solver *s, double *j);
+
+long long lbm_fluid_cells(const lbm_solver *s);
+long long lbm_steps_done(const lbm_solver *s);
+/* Device bytes the solver holds (state, masks, porosity, scratch). */
+size_t lbm_device_bytes(const lbm_solver *s);
+/* Algorithmic bytes moved per fluid lattice update: 2 * 19 * storage size. */
+double lbm_bytes_per_update(const lbm_solver *s);
+/* Number of step-kernel launches issued since creation. */
+long long lbm_launch_count(const lbm_solver *s);
+
+const char *lbm_last_error(void);
+/* Number of visible CUDA devices (0 if none or no driver). */
+int lbm_device_count(void);
+
+/* ---- host services (no GPU needed) ---- */
+
+/* LBM-Bench's geometries (src/lbm.c:52-187): "box", "channel", "pipe",
+ * "blocks[-N]", "fluid". periodic[3] is read and updated (channel, pipe and
+ * blocks force x-periodic, fluid forces all three). counts = {fluid,
+ * obstacle}. flags as above. Returns LBM_ERR_ARG for an unknown type. */
+int lbm_geometry_create(const char *type, int nx, int ny, int nz, int periodic[3], int *flags,
+    long long counts[2]);
+
+/* Porous channel: a "channel" (x-periodic, obstacle walls at y,z = 0 and
+ * n-1) plus solid spheres with seeded uniform centres (x distance taken
+ * periodically) and radii uniform in [rmin, rmax], added until the solid
+ * fraction (obstacles / all cells, walls included) reaches solid_fraction.
+ * No counterpart in the reference. */
+int lbm_porous_channel(int nx, int ny, int nz, double solid_fraction, double rmin, double rmax,
+    unsigned long long seed, int *flags, double *fraction_out, int *spheres_out);
+
+/* Seeded initial state: equilibrium of the incompressible model
+ * w_d (rho - 1.5 u.u + 3 c_d.u + 4.5 (c_d.u)^2) with density rho and
+ * u ~ U(-amplitude, amplitude)^3 per fluid cell (splitmix64); obstacle
+ * entries 0. */
+int lbm_perturbed_equilibrium(int nx, int ny, int nz, const int *flags, unsigned long long seed,
+    double amplitude, double rho, double *f);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

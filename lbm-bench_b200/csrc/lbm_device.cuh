@@ -1,0 +1,223 @@
+// Device-side building blocks of the D3Q19 TRT stream-collide-bounce-back
+// step: lattice tables, the per-cell collision, population storage codecs
+// and the orientation rules that let every propagation pattern fuse the
+// bounce-back copies of the reference into its own loads and stores.
+//
+// Reference semantics (LBM-Bench):
+//   collision      src/kernel_pull_soa.c:118-198 (identical in push and AA)
+//   bounce-back    src/lbm.c:465-568 (index lists) applied by
+//                  src/kernel_pull_soa.c:203-204, src/kernel_aa_soa.c:154-155,277-278
+//   body force     src/lbm.c:902-922, applied after every step under -DVERIFICATION
+//
+// Device layout ("plane layout"): population d of cell (x,y,z) lives at
+//   f[d * plane + (x * ny + y) * pz + z]
+// z is the unit-stride axis, as in the reference's indexSoA
+// (src/lbm.h:113-116), but without ghost cells: periodic neighbours are
+// addressed by wrapping and bounce-back links never leave the cell. pz is
+// nz rounded up so that every z-row starts on a 32-byte sector; plane is
+// nx * ny * pz rounded up to 256 bytes.
+//
+// Link mask: one 32-bit word per cell. Bit d (0..18) is set when the
+// neighbour x + c_d is an obstacle or lies outside a non-periodic axis, so
+// the population leaving along d bounces back. Bit 31 marks an obstacle
+// cell, which is never computed.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+namespace lbm {
+
+constexpr int Q = 19;
+constexpr uint32_t kSolidBit = 0x80000000u;
+
+// Reference direction order N,S,E,W,NE,SE,NW,SW,T,TN,TE,TW,TS,B,BS,BN,BW,BE,C
+// (src/lbm.h:20-38, src/lbm.c:20-29); it fixes the plane order.
+enum Dir {
+  dN = 0, dS, dE, dW, dNE, dSE, dNW, dSW, dT, dTN, dTE, dTW, dTS, dB, dBS, dBN, dBW, dBE, dC
+};
+
+__host__ __device__ constexpr int cx(int d)
+{
+  return (d == dE || d == dNE || d == dSE || d == dTE || d == dBE) ? 1
+       : (d == dW || d == dNW || d == dSW || d == dTW || d == dBW) ? -1 : 0;
+}
+__host__ __device__ constexpr int cy(int d)
+{
+  return (d == dN || d == dNE || d == dNW || d == dTN || d == dBN) ? 1
+       : (d == dS || d == dSE || d == dSW || d == dTS || d == dBS) ? -1 : 0;
+}
+__host__ __device__ constexpr int cz(int d)
+{
+  return (d == dT || d == dTN || d == dTE || d == dTW || d == dTS) ? 1
+       : (d == dB || d == dBS || d == dBN || d == dBW || d == dBE) ? -1 : 0;
+}
+__host__ __device__ constexpr int inv(int d)
+{
+  return d == dN ? dS : d == dS ? dN : d == dE ? dW : d == dW ? dE
+       : d == dNE ? dSW : d == dSW ? dNE : d == dSE ? dNW : d == dNW ? dSE
+       : d == dT ? dB : d == dB ? dT : d == dTN ? dBS : d == dBS ? dTN
+       : d == dTE ? dBW : d == dBW ? dTE : d == dTW ? dBE : d == dBE ? dTW
+       : d == dTS ? dBN : d == dBN ? dTS : dC;
+}
+// lattice weight class: 0 -> 1/3 (centre), 1 -> 1/18 (axis), 2 -> 1/36 (diagonal)
+__host__ __device__ constexpr int wclass(int d)
+{
+  return d == dC ? 0 : (cx(d) * cx(d) + cy(d) * cy(d) + cz(d) * cz(d) == 1 ? 1 : 2);
+}
+
+// Propagation patterns and the state orientations they leave behind.
+enum Pattern { kPull = 0, kPush = 1, kAA = 2 };
+enum Orientation {
+  kNatural = 0, // f_d(x) at (d, x): push state, AA after an odd step, initial AA state
+  kPullState = 1, // f_d(x) at (d, x - c_d); at (inv d, x) if x - c_d bounces
+  kAAEven = 2     // f_d(x) at (inv d, x - c_d); at (d, x) if x - c_d bounces
+};
+enum Kind { kPullStep = 0, kPushStep = 1, kAAEvenStep = 2, kAAOddStep = 3 };
+
+// Storage codecs. Value type V is what the collision computes on:
+// the population itself in FP64 mode (bit-exact reference arithmetic), the
+// shifted deviation g_d = f_d - w_d in the reduced-precision modes.
+struct StoreF64 {
+  using S = double;
+  using V = double;
+  static constexpr bool kShifted = false;
+  __device__ static V load(const S *p, int, V) { return *p; }
+  __device__ static void store(S *p, V v, V) { *p = v; }
+};
+struct StoreF32 {
+  using S = float;
+  using V = float;
+  static constexpr bool kShifted = true;
+  __device__ static V load(const S *p, int, V) { return *p; }
+  __device__ static void store(S *p, V v, V) { *p = v; }
+};
+// FP16 holds g_d * scale (scale a power of two), round-to-nearest-even.
+struct StoreF16 {
+  using S = __half;
+  using V = float;
+  static constexpr bool kShifted = true;
+  __device__ static V load(const S *p, int, V inv_scale) { return __half2float(*p) * inv_scale; }
+  __device__ static void store(S *p, V v, V scale) { *p = __float2half_rn(v * scale); }
+};
+
+template <typename V> struct Consts {
+  V omegaEven, omegaOdd;
+  V w0, w1, w2, w1X3, w1NineHalf, w2X3, w2NineHalf;
+  V force[Q];  // ((3 w_d) c_dx) F, added to every population a fluid cell receives
+  V scale;     // FP16 storage scale (1 otherwise)
+  V inv_scale;
+  V alpha;     // Brinkman coefficient scale
+};
+
+// One cell's TRT collision (src/kernel_pull_soa.c:118-198), operation for
+// operation in the reference's order; FP64 translation units are compiled
+// with --fmad=false so no multiply-add is contracted. In the shifted modes
+// the same formulas hold with f -> g and rho -> rho - 1 because the shift is
+// the rest equilibrium w_d. kappa != 0 adds the Brinkman resistance
+// F_b = -kappa u as 3 w_d c_d . F_b = -/+ kappa (c_d . u) 3 w_d on each pair.
+template <typename V, bool BRINK>
+__device__ __forceinline__ void collide(const V (&f)[Q], V (&o)[Q], const Consts<V> &c, V kappa,
+    V *u_out = nullptr)
+{
+  const V ux = f[dE] + f[dNE] + f[dSE] + f[dTE] + f[dBE] - f[dW] - f[dNW] - f[dSW] - f[dTW] - f[dBW];
+  const V uy = f[dN] + f[dNE] + f[dNW] + f[dTN] + f[dBN] - f[dS] - f[dSE] - f[dSW] - f[dTS] - f[dBS];
+  const V uz = f[dT] + f[dTE] + f[dTW] + f[dTN] + f[dTS] - f[dB] - f[dBE] - f[dBW] - f[dBN] - f[dBS];
+  const V dens = f[dC] + f[dN] + f[dE] + f[dS] + f[dW] + f[dNE] + f[dSE] + f[dSW] + f[dNW] + f[dT] +
+                 f[dTN] + f[dTE] + f[dTS] + f[dTW] + f[dB] + f[dBN] + f[dBE] + f[dBS] + f[dBW];
+  const V dirIndepTrm = dens - (ux * ux + uy * uy + uz * uz) * V(3.0) / V(2.0);
+  if (u_out) {
+    u_out[0] = ux;
+    u_out[1] = uy;
+    u_out[2] = uz;
+  }
+  const V oE = c.omegaEven, oO = c.omegaOdd;
+  o[dC] = f[dC] - oE * (f[dC] - c.w0 * dirIndepTrm);
+  const V w1Indep = c.w1 * dirIndepTrm;
+  const V w2Indep = c.w2 * dirIndepTrm;
+
+  auto pair = [&](int a, int b, V ui, V wnh, V wx3, V windep) {
+    const V evenPart = oE * (V(0.5) * (f[a] + f[b]) - ui * ui * wnh - windep);
+    const V oddPart = oO * (V(0.5) * (f[a] - f[b]) - ui * wx3);
+    if (BRINK) {
+      const V bterm = kappa * ui * wx3;
+      o[a] = f[a] - evenPart - oddPart - bterm;
+      o[b] = f[b] - evenPart + oddPart + bterm;
+    } else {
+      o[a] = f[a] - evenPart - oddPart;
+      o[b] = f[b] - evenPart + oddPart;
+    }
+  };
+  pair(dN, dS, uy, c.w1NineHalf, c.w1X3, w1Indep);
+  pair(dE, dW, ux, c.w1NineHalf, c.w1X3, w1Indep);
+  pair(dT, dB, uz, c.w1NineHalf, c.w1X3, w1Indep);
+  pair(dNW, dSE, -ux + uy, c.w2NineHalf, c.w2X3, w2Indep);
+  pair(dNE, dSW, ux + uy, c.w2NineHalf, c.w2X3, w2Indep);
+  pair(dTW, dBE, -ux + uz, c.w2NineHalf, c.w2X3, w2Indep);
+  pair(dTE, dBW, ux + uz, c.w2NineHalf, c.w2X3, w2Indep);
+  pair(dTS, dBN, -uy + uz, c.w2NineHalf, c.w2X3, w2Indep);
+  pair(dTN, dBS, uy + uz, c.w2NineHalf, c.w2X3, w2Indep);
+}
+
+// Geometry of the device lattice, passed by value to every kernel.
+struct Grid {
+  int nx, ny, nz, pz;
+  long long plane; // elements per direction plane
+};
+
+// Cell coordinates -> cell index in the plane layout.
+__device__ __forceinline__ long long cell_index(const Grid &g, int x, int y, int z)
+{
+  return ((long long)x * g.ny + y) * g.pz + z;
+}
+
+// The 3x3x3 wrapped neighbourhood of a cell, from which each direction's
+// neighbour index is one add. Wrapping happens on every axis: a link that
+// leaves a non-periodic axis is flagged in the mask and never dereferenced.
+struct Nbhd {
+  long long row[3][3]; // row[cx+1][cy+1] = (x' * ny + y') * pz
+  int zz[3];           // z', for cz = -1, 0, 1
+  __device__ __forceinline__ long long at(int d) const
+  {
+    return row[cx(d) + 1][cy(d) + 1] + zz[cz(d) + 1];
+  }
+};
+
+__device__ __forceinline__ Nbhd make_nbhd(const Grid &g, int x, int y, int z)
+{
+  Nbhd n;
+  const int xs[3] = { x == 0 ? g.nx - 1 : x - 1, x, x == g.nx - 1 ? 0 : x + 1 };
+  const int ys[3] = { y == 0 ? g.ny - 1 : y - 1, y, y == g.ny - 1 ? 0 : y + 1 };
+  n.zz[0] = z == 0 ? g.nz - 1 : z - 1;
+  n.zz[1] = z;
+  n.zz[2] = z == g.nz - 1 ? 0 : z + 1;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+      n.row[a][b] = ((long long)xs[a] * g.ny + ys[b]) * g.pz;
+  return n;
+}
+
+// Neighbour x - c_d is the neighbour x + c_{inv d}.
+__device__ __forceinline__ long long behind(const Nbhd &n, int d) { return n.at(inv(d)); }
+
+// Where f_d(x) of fluid cell x lives in a state of orientation `o`:
+// plane index and cell index.
+__device__ __forceinline__ void state_slot(int o, int d, uint32_t mask, long long cell,
+    const Nbhd &n, int &plane_out, long long &cell_out)
+{
+  const bool bounced = (mask >> inv(d)) & 1u; // x - c_d is a wall
+  if (o == kNatural) {
+    plane_out = d;
+    cell_out = cell;
+  } else if (o == kPullState) {
+    plane_out = bounced ? inv(d) : d;
+    cell_out = bounced ? cell : behind(n, d);
+  } else {
+    plane_out = bounced ? d : inv(d);
+    cell_out = bounced ? cell : behind(n, d);
+  }
+}
+
+} // namespace lbm

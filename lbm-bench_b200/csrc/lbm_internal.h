@@ -1,0 +1,34 @@
+// Internal interfaces between the translation units of liblbmb200.so.
+// Not installed; the public C ABI is include/lbm_b200.h.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "lbm_step.cuh"
+
+namespace lbm {
+
+enum Precision { kF64 = 0, kF32 = 1, kF16 = 2 };
+
+// Step launchers, one per storage type (lbm_step_f64.cu is compiled with
+// --fmad=false for bit-exact reference arithmetic; lbm_step_lp.cu is not).
+cudaError_t launch_step_f64(int kind, bool force, bool brink, const StepArgs<StoreF64> &a,
+    dim3 grid, dim3 block, cudaStream_t st);
+cudaError_t launch_step_f32(int kind, bool force, bool brink, const StepArgs<StoreF32> &a,
+    dim3 grid, dim3 block, cudaStream_t st);
+cudaError_t launch_step_f16(int kind, bool force, bool brink, const StepArgs<StoreF16> &a,
+    dim3 grid, dim3 block, cudaStream_t st);
+
+// Block/grid shape of the per-cell kernels: z across lanes, then y, one
+// x-plane per grid.z.
+inline void cell_launch_shape(const Grid &g, dim3 &grid, dim3 &block)
+{
+  int tz = 32;
+  while (tz < g.nz && tz < kStepThreads)
+    tz *= 2;
+  int ty = kStepThreads / tz;
+  block = dim3(tz, ty, 1);
+  grid = dim3((g.nz + tz - 1) / tz, (g.ny + ty - 1) / ty, g.nx);
+}
+
+} // namespace lbm

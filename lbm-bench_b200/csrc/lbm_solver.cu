@@ -1,0 +1,1020 @@
+// liblbmb200: solver object and flat C ABI (include/lbm_b200.h).
+//
+// Replaces, for the SoA pull/push/AA kernels of LBM-Bench:
+//   kernelInitInternal (src/lbm.c:400-599)  -> lbm_create: device buffers
+//     and a per-cell link mask instead of bounce-back index lists;
+//   kd->Kernel time loops (src/kernel_{pull,push,aa}_soa.c)  -> lbm_run;
+//   Get/SetNode (src/lbm.c:193-294)  -> lbm_get_state / lbm_set_state,
+//     converting between the caller's f[d][x][y][z] and the device
+//     orientation of the pattern;
+//   kernelDensity (src/lbm.c:928-947)  -> lbm_mass_momentum (FP64, on device);
+//   kernelDeinit (src/lbm.c:660-670)  -> lbm_destroy.
+// There is no CPU path: without a CUDA device every call that needs one
+// fails with LBM_ERR_NODEV.
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "lbm_b200.h"
+#include "lbm_internal.h"
+
+using namespace lbm;
+
+static thread_local char g_err[512] = "";
+
+static int fail(int code, const char *fmt, ...)
+{
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CUDA_TRY(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return fail(e_ == cudaErrorMemoryAllocation ? LBM_ERR_ALLOC : LBM_ERR_CUDA,          \
+          "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);     \
+  } while (0)
+
+struct lbm_solver {
+  int nx, ny, nz;
+  int periodic[3];
+  int pattern, precision;
+  Grid g;
+  int device;
+  cudaStream_t stream;
+  cudaEvent_t ev[2];
+  void *buf[2];
+  size_t state_bytes;
+  int cur; // pull/push: buffer holding the state
+  long long steps_done;
+  uint32_t *mask;
+  float *porosity;
+  double alpha;
+  double *staging; // one dense plane, nx*ny*nz doubles
+  double *red;     // reduction partials
+  long long n_fluid;
+  double omega, lambda, xforce;
+  int force_on;
+  double fp16_scale;
+  long long launches;
+  size_t dev_bytes;
+};
+
+extern "C" const char *lbm_last_error(void) { return g_err; }
+
+extern "C" int lbm_device_count(void)
+{
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+static size_t storage_size(int precision)
+{
+  return precision == LBM_F64 ? 8 : precision == LBM_F32 ? 4 : 2;
+}
+
+static int orientation(const lbm_solver *s)
+{
+  if (s->pattern == LBM_PULL)
+    return kPullState;
+  if (s->pattern == LBM_PUSH)
+    return kNatural;
+  return (s->steps_done & 1) ? kAAEven : kNatural;
+}
+
+// Lattice weights by direction.
+static double weight(int d)
+{
+  int c = wclass(d);
+  return c == 0 ? 1.0 / 3.0 : c == 1 ? 1.0 / 18.0 : 1.0 / 36.0;
+}
+
+// Kernel constants, computed in double exactly as the reference does
+// (src/kernel_pull_soa.c:18-28, src/lbm.c:904-919) and rounded to V.
+template <typename V> static Consts<V> make_consts(const lbm_solver *s)
+{
+  Consts<V> c;
+  const double w0 = 1.0 / 3.0, w1 = 1.0 / 18.0, w2 = 1.0 / 36.0;
+  c.omegaEven  = (V)s->omega;
+  c.omegaOdd   = (V)(1.0 / (0.5 + s->lambda / (1.0 / s->omega - 0.5)));
+  c.w0         = (V)w0;
+  c.w1         = (V)w1;
+  c.w2         = (V)w2;
+  c.w1X3       = (V)(w1 * 3.0);
+  c.w1NineHalf = (V)(w1 * 9.0 / 2.0);
+  c.w2X3       = (V)(w2 * 3.0);
+  c.w2NineHalf = (V)(w2 * 9.0 / 2.0);
+  for (int d = 0; d < Q; ++d)
+    c.force[d] = (V)(3.0 * weight(d) * (double)cx(d) * s->xforce);
+  c.scale     = (V)(s->precision == LBM_F16 ? s->fp16_scale : 1.0);
+  c.inv_scale = (V)(s->precision == LBM_F16 ? 1.0 / s->fp16_scale : 1.0);
+  c.alpha     = (V)s->alpha;
+  return c;
+}
+
+// ---------------------------------------------------------------------------
+// Auxiliary kernels
+// ---------------------------------------------------------------------------
+
+// One thread per cell of the padded box (z < pz); cells with z >= nz are
+// padding and are marked solid.
+__global__ void mask_kernel(Grid g, int px, int py, int pz, const uint8_t *fluid, uint32_t *mask)
+{
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= g.pz || y >= g.ny)
+    return;
+  const long long cell = cell_index(g, x, y, z);
+  if (z >= g.nz || !fluid[cell]) {
+    mask[cell] = kSolidBit;
+    return;
+  }
+  uint32_t m = 0;
+#pragma unroll
+  for (int d = 0; d < Q; ++d) {
+    int a = x + cx(d), b = y + cy(d), c = z + cz(d);
+    bool wall = false;
+    if (a < 0 || a >= g.nx) {
+      if (px)
+        a = a < 0 ? g.nx - 1 : 0;
+      else
+        wall = true;
+    }
+    if (b < 0 || b >= g.ny) {
+      if (py)
+        b = b < 0 ? g.ny - 1 : 0;
+      else
+        wall = true;
+    }
+    if (c < 0 || c >= g.nz) {
+      if (pz)
+        c = c < 0 ? g.nz - 1 : 0;
+      else
+        wall = true;
+    }
+    if (!wall && !fluid[cell_index(g, a, b, c)])
+      wall = true;
+    if (wall)
+      m |= 1u << d;
+  }
+  mask[cell] = m;
+}
+
+__device__ __forceinline__ long long dense_index(const Grid &g, int x, int y, int z)
+{
+  return ((long long)x * g.ny + y) * g.nz + z;
+}
+
+// Dense plane d (caller layout) -> device state in orientation `orient`.
+template <class ST>
+__global__ void pack_plane_kernel(Grid g, int d, int orient, const double *__restrict__ dense,
+    typename ST::S *state, const uint32_t *__restrict__ mask, float scale, double wd)
+{
+  using V = typename ST::V;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= g.nz || y >= g.ny)
+    return;
+  const long long cell = cell_index(g, x, y, z);
+  const uint32_t m = mask[cell];
+  if (m & kSolidBit)
+    return;
+  Nbhd nb = make_nbhd(g, x, y, z);
+  int p;
+  long long c;
+  state_slot(orient, d, m, cell, nb, p, c);
+  double v = dense[dense_index(g, x, y, z)];
+  if (ST::kShifted)
+    v -= wd;
+  ST::store(state + (long long)p * g.plane + c, (V)v, (V)scale);
+}
+
+// Device state -> dense plane d (caller layout); obstacles get 0.
+template <class ST>
+__global__ void unpack_plane_kernel(Grid g, int d, int orient, double *__restrict__ dense,
+    const typename ST::S *state, const uint32_t *__restrict__ mask, float inv_scale, double wd)
+{
+  using V = typename ST::V;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= g.nz || y >= g.ny)
+    return;
+  const long long cell = cell_index(g, x, y, z);
+  const uint32_t m = mask[cell];
+  if (m & kSolidBit) {
+    dense[dense_index(g, x, y, z)] = 0.0;
+    return;
+  }
+  Nbhd nb = make_nbhd(g, x, y, z);
+  int p;
+  long long c;
+  state_slot(orient, d, m, cell, nb, p, c);
+  double v = (double)ST::load(state + (long long)p * g.plane + c, d, (V)inv_scale);
+  if (ST::kShifted)
+    v += wd;
+  dense[dense_index(g, x, y, z)] = v;
+}
+
+// Density and momentum of one fluid cell in FP64. For shifted storage the
+// density is 1 + sum g (the shift sums to 1, its first moment to 0).
+template <class ST>
+__device__ __forceinline__ void cell_moments(const Grid &g, const typename ST::S *state,
+    int orient, uint32_t m, long long cell, const Nbhd &nb, float inv_scale, double &rho,
+    double &jx, double &jy, double &jz, bool &finite)
+{
+  using V = typename ST::V;
+  rho = ST::kShifted ? 1.0 : 0.0;
+  jx = jy = jz = 0.0;
+  finite = true;
+#pragma unroll
+  for (int d = 0; d < Q; ++d) {
+    int p;
+    long long c;
+    state_slot(orient, d, m, cell, nb, p, c);
+    const double v = (double)ST::load(state + (long long)p * g.plane + c, d, (V)inv_scale);
+    finite = finite && isfinite(v);
+    rho += v;
+    jx += cx(d) * v;
+    jy += cy(d) * v;
+    jz += cz(d) * v;
+  }
+}
+
+// quantity: 0 rho, 1 ux, 2 uy, 3 uz (momentum) -> dense cell array
+template <class ST>
+__global__ void moments_kernel(Grid g, int orient, int quantity, const typename ST::S *state,
+    const uint32_t *__restrict__ mask, float inv_scale, double *out)
+{
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= g.nz || y >= g.ny)
+    return;
+  const long long cell = cell_index(g, x, y, z);
+  const uint32_t m = mask[cell];
+  double r = 0.0;
+  if (!(m & kSolidBit)) {
+    Nbhd nb = make_nbhd(g, x, y, z);
+    double rho, jx, jy, jz;
+    bool fin;
+    cell_moments<ST>(g, state, orient, m, cell, nb, inv_scale, rho, jx, jy, jz, fin);
+    r = quantity == 0 ? rho : quantity == 1 ? jx : quantity == 2 ? jy : jz;
+  }
+  out[dense_index(g, x, y, z)] = r;
+}
+
+constexpr int kRedThreads = 256;
+constexpr int kRedBlocks = 592; // 4 per SM on a 148-SM B200; fixed for determinism
+constexpr int kRedVals = 6;
+
+// Fixed-shape tree reduction of kRedVals doubles inside one block.
+// ops: bit k set -> value k is reduced with max instead of +.
+__device__ void block_reduce(double (&v)[kRedVals], double *out, unsigned ops)
+{
+  __shared__ double sh[kRedVals][kRedThreads];
+  for (int k = 0; k < kRedVals; ++k)
+    sh[k][threadIdx.x] = v[k];
+  __syncthreads();
+  for (int s = kRedThreads / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s)
+      for (int k = 0; k < kRedVals; ++k) {
+        double a = sh[k][threadIdx.x], b = sh[k][threadIdx.x + s];
+        sh[k][threadIdx.x] = ((ops >> k) & 1u) ? fmax(a, b) : a + b;
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < kRedVals; ++k)
+      out[k] = sh[k][0];
+}
+
+// Per-block partial sums over cells i = blockIdx.x*T + threadIdx.x + k*grid*T
+// of the dense box: mass, jx, jy, jz, non-finite cells.
+template <class ST>
+__global__ void __launch_bounds__(kRedThreads) mass_kernel(Grid g, int orient,
+    const typename ST::S *state, const uint32_t *__restrict__ mask, float inv_scale,
+    double *partial)
+{
+  double v[kRedVals] = { 0, 0, 0, 0, 0, 0 };
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long i = (long long)blockIdx.x * kRedThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kRedThreads) {
+    const int z = (int)(i % g.nz);
+    const long long r = i / g.nz;
+    const int y = (int)(r % g.ny);
+    const int x = (int)(r / g.ny);
+    const long long cell = cell_index(g, x, y, z);
+    const uint32_t m = mask[cell];
+    if (m & kSolidBit)
+      continue;
+    Nbhd nb = make_nbhd(g, x, y, z);
+    double rho, jx, jy, jz;
+    bool fin;
+    cell_moments<ST>(g, state, orient, m, cell, nb, inv_scale, rho, jx, jy, jz, fin);
+    v[0] += rho;
+    v[1] += jx;
+    v[2] += jy;
+    v[3] += jz;
+    v[4] += fin ? 0.0 : 1.0;
+  }
+  block_reduce(v, partial + (size_t)blockIdx.x * kRedVals, 0u);
+}
+
+// Sum (or max, per ops) of nblocks partial rows in a fixed order.
+__global__ void __launch_bounds__(kRedThreads) final_reduce_kernel(const double *partial,
+    int nblocks, unsigned ops, double *out)
+{
+  double v[kRedVals];
+  for (int k = 0; k < kRedVals; ++k)
+    v[k] = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += kRedThreads)
+    for (int k = 0; k < kRedVals; ++k) {
+      double x = partial[(size_t)b * kRedVals + k];
+      v[k] = ((ops >> k) & 1u) ? fmax(v[k], x) : v[k] + x;
+    }
+  block_reduce(v, out, ops);
+}
+
+// Velocity/density differences of two states over the same geometry.
+template <class SA, class SB>
+__global__ void __launch_bounds__(kRedThreads) compare_kernel(Grid ga, Grid gb, int oa, int ob,
+    const typename SA::S *sa, const typename SB::S *sb, const uint32_t *__restrict__ mask_a,
+    const uint32_t *__restrict__ mask_b, float inv_a, float inv_b, double *partial)
+{
+  double v[kRedVals] = { 0, 0, 0, 0, 0, 0 };
+  const long long n = (long long)ga.nx * ga.ny * ga.nz;
+  for (long long i = (long long)blockIdx.x * kRedThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kRedThreads) {
+    const int z = (int)(i % ga.nz);
+    const long long r = i / ga.nz;
+    const int y = (int)(r % ga.ny);
+    const int x = (int)(r / ga.ny);
+    const long long ca = cell_index(ga, x, y, z), cb = cell_index(gb, x, y, z);
+    const uint32_t ma = mask_a[ca], mb = mask_b[cb];
+    if ((ma & kSolidBit) || (mb & kSolidBit))
+      continue;
+    Nbhd na = make_nbhd(ga, x, y, z), nbb = make_nbhd(gb, x, y, z);
+    double ra, xa, ya, za, rb, xb, yb, zb;
+    bool fa, fb;
+    cell_moments<SA>(ga, sa, oa, ma, ca, na, inv_a, ra, xa, ya, za, fa);
+    cell_moments<SB>(gb, sb, ob, mb, cb, nbb, inv_b, rb, xb, yb, zb, fb);
+    const double dx = xa - xb, dy = ya - yb, dz = za - zb, dr = ra - rb;
+    const double du2 = dx * dx + dy * dy + dz * dz, ub2 = xb * xb + yb * yb + zb * zb;
+    v[0] += du2;
+    v[1] += ub2;
+    v[2] += dr * dr;
+    v[3] += rb * rb;
+    v[4] = fmax(v[4], sqrt(du2));
+    v[5] = fmax(v[5], sqrt(ub2));
+  }
+  block_reduce(v, partial + (size_t)blockIdx.x * kRedVals, 0x30u);
+}
+
+// Sum of the x momentum and fluid count over the plane x = nx-1.
+template <class ST>
+__global__ void __launch_bounds__(kRedThreads) outlet_kernel(Grid g, int orient,
+    const typename ST::S *state, const uint32_t *__restrict__ mask, float inv_scale,
+    double *partial)
+{
+  double v[kRedVals] = { 0, 0, 0, 0, 0, 0 };
+  const long long n = (long long)g.ny * g.nz;
+  const int x = g.nx - 1;
+  for (long long i = (long long)blockIdx.x * kRedThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kRedThreads) {
+    const int z = (int)(i % g.nz);
+    const int y = (int)(i / g.nz);
+    const long long cell = cell_index(g, x, y, z);
+    const uint32_t m = mask[cell];
+    if (m & kSolidBit)
+      continue;
+    Nbhd nb = make_nbhd(g, x, y, z);
+    double rho, jx, jy, jz;
+    bool fin;
+    cell_moments<ST>(g, state, orient, m, cell, nb, inv_scale, rho, jx, jy, jz, fin);
+    v[0] += jx;
+    v[1] += 1.0;
+  }
+  block_reduce(v, partial + (size_t)blockIdx.x * kRedVals, 0u);
+}
+
+// ---------------------------------------------------------------------------
+// Helpers
+// ---------------------------------------------------------------------------
+
+static const void *state_ptr(const lbm_solver *s)
+{
+  return s->pattern == LBM_AA ? s->buf[0] : s->buf[s->cur];
+}
+
+static int need_device(void)
+{
+  if (lbm_device_count() <= 0)
+    return fail(LBM_ERR_NODEV, "no CUDA device visible; liblbmb200 has no CPU path");
+  return LBM_OK;
+}
+
+static void free_all(lbm_solver *s)
+{
+  if (!s)
+    return;
+  cudaFree(s->buf[0]);
+  cudaFree(s->buf[1]);
+  cudaFree(s->mask);
+  cudaFree(s->porosity);
+  cudaFree(s->staging);
+  cudaFree(s->red);
+  if (s->ev[0])
+    cudaEventDestroy(s->ev[0]);
+  if (s->ev[1])
+    cudaEventDestroy(s->ev[1]);
+  if (s->stream)
+    cudaStreamDestroy(s->stream);
+  free(s);
+}
+
+static int dev_alloc(lbm_solver *s, void **p, size_t bytes, const char *what)
+{
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = NULL;
+    return fail(e == cudaErrorMemoryAllocation ? LBM_ERR_ALLOC : LBM_ERR_CUDA,
+        "cudaMalloc of %.3f GB for %s failed: %s", bytes / 1e9, what, cudaGetErrorString(e));
+  }
+  s->dev_bytes += bytes;
+  return LBM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *flags,
+    int periodic_x, int periodic_y, int periodic_z, int pattern, int precision)
+{
+  if (!out)
+    return fail(LBM_ERR_ARG, "lbm_create: out is NULL");
+  *out = NULL;
+  if (nx <= 0 || ny <= 0 || nz <= 0 || !flags)
+    return fail(LBM_ERR_ARG, "lbm_create: bad dimensions %dx%dx%d or NULL flags", nx, ny, nz);
+  if (pattern != LBM_PULL && pattern != LBM_PUSH && pattern != LBM_AA)
+    return fail(LBM_ERR_ARG, "lbm_create: unknown pattern %d", pattern);
+  if (precision != LBM_F64 && precision != LBM_F32 && precision != LBM_F16)
+    return fail(LBM_ERR_ARG, "lbm_create: unknown precision %d", precision);
+  if (nx > 65535)
+    return fail(LBM_ERR_ARG, "lbm_create: nx = %d exceeds 65535 (one grid.z slice per x)", nx);
+  int rc = need_device();
+  if (rc)
+    return rc;
+
+  lbm_solver *s = (lbm_solver *)calloc(1, sizeof(lbm_solver));
+  if (!s)
+    return fail(LBM_ERR_ALLOC, "lbm_create: host allocation failed");
+  s->nx = nx;
+  s->ny = ny;
+  s->nz = nz;
+  s->periodic[0] = periodic_x ? 1 : 0;
+  s->periodic[1] = periodic_y ? 1 : 0;
+  s->periodic[2] = periodic_z ? 1 : 0;
+  s->pattern = pattern;
+  s->precision = precision;
+  s->omega = 1.0;
+  s->lambda = 1.0 / 12.0;
+  s->xforce = 1e-5;
+  s->force_on = 0;
+  s->fp16_scale = 16384.0;
+  cudaGetDevice(&s->device);
+
+  const size_t S = storage_size(precision);
+  const int zq = (int)(32 / S); // z pitch quantum: rows start on a 32-byte sector
+  s->g.nx = nx;
+  s->g.ny = ny;
+  s->g.nz = nz;
+  s->g.pz = (nz + zq - 1) / zq * zq;
+  long long cells = (long long)nx * ny * s->g.pz;
+  const long long pq = 256 / (long long)S;
+  s->g.plane = (cells + pq - 1) / pq * pq;
+  s->state_bytes = (size_t)Q * (size_t)s->g.plane * S;
+
+#define TRY(x)                                                                              \
+  do {                                                                                      \
+    int r_ = (x);                                                                           \
+    if (r_) {                                                                               \
+      free_all(s);                                                                          \
+      return r_;                                                                            \
+    }                                                                                       \
+  } while (0)
+#define TRYC(x)                                                                             \
+  do {                                                                                      \
+    cudaError_t e_ = (x);                                                                   \
+    if (e_ != cudaSuccess) {                                                                \
+      free_all(s);                                                                          \
+      return fail(LBM_ERR_CUDA, "%s failed: %s", #x, cudaGetErrorString(e_));               \
+    }                                                                                       \
+  } while (0)
+
+  TRYC(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  TRYC(cudaEventCreate(&s->ev[0]));
+  TRYC(cudaEventCreate(&s->ev[1]));
+  TRY(dev_alloc(s, &s->buf[0], s->state_bytes, "the population lattice"));
+  if (pattern != LBM_AA)
+    TRY(dev_alloc(s, &s->buf[1], s->state_bytes, "the second population lattice"));
+  TRY(dev_alloc(s, (void **)&s->mask, (size_t)s->g.plane * 4, "the link masks"));
+  TRY(dev_alloc(s, (void **)&s->staging, sizeof(double) * (size_t)nx * ny * nz,
+      "the transfer plane"));
+  TRY(dev_alloc(s, (void **)&s->red, sizeof(double) * kRedVals * (kRedBlocks + 1),
+      "reduction partials"));
+  TRYC(cudaMemsetAsync(s->buf[0], 0, s->state_bytes, s->stream));
+  if (s->buf[1])
+    TRYC(cudaMemsetAsync(s->buf[1], 0, s->state_bytes, s->stream));
+
+  // fluid bytes in device cell order (padding = solid), then the masks
+  std::vector<uint8_t> fluid((size_t)cells, 0);
+  long long nf = 0;
+  for (int x = 0; x < nx; ++x)
+    for (int y = 0; y < ny; ++y)
+      for (int z = 0; z < nz; ++z) {
+        uint8_t f = flags[((long long)z * ny + y) * nx + x] != 0;
+        fluid[((size_t)x * ny + y) * s->g.pz + z] = f;
+        nf += f;
+      }
+  s->n_fluid = nf;
+  uint8_t *dfluid = NULL;
+  TRYC(cudaMalloc((void **)&dfluid, (size_t)cells));
+  cudaError_t e = cudaMemcpyAsync(dfluid, fluid.data(), (size_t)cells, cudaMemcpyHostToDevice,
+      s->stream);
+  if (e == cudaSuccess) {
+    Grid gp = s->g;
+    gp.nz = s->g.pz; // cover the padding too
+    dim3 grid, block;
+    cell_launch_shape(gp, grid, block);
+    mask_kernel<<<grid, block, 0, s->stream>>>(s->g, s->periodic[0], s->periodic[1],
+        s->periodic[2], dfluid, s->mask);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(s->stream);
+  cudaFree(dfluid);
+  if (e != cudaSuccess) {
+    free_all(s);
+    return fail(LBM_ERR_CUDA, "lbm_create: mask build failed: %s", cudaGetErrorString(e));
+  }
+  // cells beyond nx*ny*pz inside the rounded plane stay unused; mark them solid
+  // so no kernel that walks the whole plane ever treats them as fluid
+  if (s->g.plane > cells) {
+    std::vector<uint32_t> pad((size_t)(s->g.plane - cells), kSolidBit);
+    TRYC(cudaMemcpy(s->mask + cells, pad.data(), pad.size() * 4, cudaMemcpyHostToDevice));
+  }
+#undef TRY
+#undef TRYC
+  *out = s;
+  return LBM_OK;
+}
+
+extern "C" int lbm_destroy(lbm_solver *s)
+{
+  if (!s)
+    return LBM_OK;
+  cudaStreamSynchronize(s->stream);
+  free_all(s);
+  return LBM_OK;
+}
+
+extern "C" int lbm_set_params(lbm_solver *s, double omega, double lambda, double xforce,
+    int force_on)
+{
+  if (!s)
+    return fail(LBM_ERR_ARG, "lbm_set_params: NULL solver");
+  if (!(omega > 0.0 && omega < 2.0))
+    return fail(LBM_ERR_ARG, "lbm_set_params: omega = %g outside (0, 2)", omega);
+  if (!(lambda > 0.0) || !isfinite(xforce))
+    return fail(LBM_ERR_ARG, "lbm_set_params: bad Lambda %g or force %g", lambda, xforce);
+  s->omega = omega;
+  s->lambda = lambda;
+  s->xforce = xforce;
+  s->force_on = force_on ? 1 : 0;
+  return LBM_OK;
+}
+
+extern "C" int lbm_set_fp16_scale(lbm_solver *s, double scale)
+{
+  if (!s || s->precision != LBM_F16)
+    return fail(LBM_ERR_ARG, "lbm_set_fp16_scale: not an FP16 solver");
+  int ex;
+  if (!(scale > 0.0) || frexp(scale, &ex) != 0.5)
+    return fail(LBM_ERR_ARG, "lbm_set_fp16_scale: %g is not a power of two", scale);
+  s->fp16_scale = scale;
+  return LBM_OK;
+}
+
+extern "C" int lbm_set_porosity(lbm_solver *s, const float *porosity, double alpha)
+{
+  if (!s)
+    return fail(LBM_ERR_ARG, "lbm_set_porosity: NULL solver");
+  if (alpha == 0.0) {
+    s->alpha = 0.0;
+    return LBM_OK;
+  }
+  if (!porosity || !(alpha > 0.0))
+    return fail(LBM_ERR_ARG, "lbm_set_porosity: NULL porosity or alpha %g <= 0", alpha);
+  if (!s->porosity) {
+    int rc = dev_alloc(s, (void **)&s->porosity, sizeof(float) * (size_t)s->g.plane,
+        "the porosity field");
+    if (rc)
+      return rc;
+    CUDA_TRY(cudaMemsetAsync(s->porosity, 0, sizeof(float) * (size_t)s->g.plane, s->stream));
+  }
+  for (int x = 0; x < s->nx; ++x)
+    for (int y = 0; y < s->ny; ++y)
+      CUDA_TRY(cudaMemcpyAsync(s->porosity + ((size_t)x * s->ny + y) * s->g.pz,
+          porosity + ((size_t)x * s->ny + y) * s->nz, sizeof(float) * s->nz,
+          cudaMemcpyHostToDevice, s->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  s->alpha = alpha;
+  return LBM_OK;
+}
+
+template <class ST> static int pack_all(lbm_solver *s, const double *f)
+{
+  dim3 grid, block;
+  cell_launch_shape(s->g, grid, block);
+  const int o = orientation(s);
+  const size_t plane_host = (size_t)s->nx * s->ny * s->nz;
+  using Sx = typename ST::S;
+  Sx *state = (Sx *)state_ptr(s);
+  for (int d = 0; d < Q; ++d) {
+    CUDA_TRY(cudaMemcpyAsync(s->staging, f + d * plane_host, sizeof(double) * plane_host,
+        cudaMemcpyHostToDevice, s->stream));
+    pack_plane_kernel<ST><<<grid, block, 0, s->stream>>>(s->g, d, o, s->staging, state, s->mask,
+        (float)(s->precision == LBM_F16 ? s->fp16_scale : 1.0), weight(d));
+    CUDA_TRY(cudaGetLastError());
+  }
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return LBM_OK;
+}
+
+template <class ST> static int unpack_all(lbm_solver *s, double *f)
+{
+  dim3 grid, block;
+  cell_launch_shape(s->g, grid, block);
+  const int o = orientation(s);
+  const size_t plane_host = (size_t)s->nx * s->ny * s->nz;
+  using Sx = typename ST::S;
+  const Sx *state = (const Sx *)state_ptr(s);
+  for (int d = 0; d < Q; ++d) {
+    unpack_plane_kernel<ST><<<grid, block, 0, s->stream>>>(s->g, d, o, s->staging, state,
+        s->mask, (float)(s->precision == LBM_F16 ? 1.0 / s->fp16_scale : 1.0), weight(d));
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(f + d * plane_host, s->staging, sizeof(double) * plane_host,
+        cudaMemcpyDeviceToHost, s->stream));
+  }
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return LBM_OK;
+}
+
+extern "C" int lbm_set_state(lbm_solver *s, const double *f)
+{
+  if (!s || !f)
+    return fail(LBM_ERR_ARG, "lbm_set_state: NULL argument");
+  CUDA_TRY(cudaSetDevice(s->device));
+  switch (s->precision) {
+  case LBM_F64: return pack_all<StoreF64>(s, f);
+  case LBM_F32: return pack_all<StoreF32>(s, f);
+  default: return pack_all<StoreF16>(s, f);
+  }
+}
+
+extern "C" int lbm_get_state(lbm_solver *s, double *f)
+{
+  if (!s || !f)
+    return fail(LBM_ERR_ARG, "lbm_get_state: NULL argument");
+  CUDA_TRY(cudaSetDevice(s->device));
+  switch (s->precision) {
+  case LBM_F64: return unpack_all<StoreF64>(s, f);
+  case LBM_F32: return unpack_all<StoreF32>(s, f);
+  default: return unpack_all<StoreF16>(s, f);
+  }
+}
+
+// Launches one step and advances the bookkeeping.
+static int launch_one(lbm_solver *s, int *kind_out)
+{
+  dim3 grid, block;
+  cell_launch_shape(s->g, grid, block);
+  int kind;
+  const void *src;
+  void *dst;
+  if (s->pattern == LBM_AA) {
+    kind = (s->steps_done & 1) ? kAAOddStep : kAAEvenStep;
+    src = dst = s->buf[0];
+  } else {
+    kind = s->pattern == LBM_PULL ? kPullStep : kPushStep;
+    src = s->buf[s->cur];
+    dst = s->buf[s->cur ^ 1];
+  }
+  const bool brink = s->alpha != 0.0 && s->porosity;
+  const bool force = s->force_on || brink;
+  cudaError_t e;
+  if (s->precision == LBM_F64) {
+    StepArgs<StoreF64> a;
+    a.g = s->g;
+    a.src = (const double *)src;
+    a.dst = (double *)dst;
+    a.mask = s->mask;
+    a.porosity = s->porosity;
+    a.u_save = nullptr;
+    a.c = make_consts<double>(s);
+    e = launch_step_f64(kind, force, brink, a, grid, block, s->stream);
+  } else if (s->precision == LBM_F32) {
+    StepArgs<StoreF32> a;
+    a.g = s->g;
+    a.src = (const float *)src;
+    a.dst = (float *)dst;
+    a.mask = s->mask;
+    a.porosity = s->porosity;
+    a.u_save = nullptr;
+    a.c = make_consts<float>(s);
+    e = launch_step_f32(kind, force, brink, a, grid, block, s->stream);
+  } else {
+    StepArgs<StoreF16> a;
+    a.g = s->g;
+    a.src = (const __half *)src;
+    a.dst = (__half *)dst;
+    a.mask = s->mask;
+    a.porosity = s->porosity;
+    a.u_save = nullptr;
+    a.c = make_consts<float>(s);
+    e = launch_step_f16(kind, force, brink, a, grid, block, s->stream);
+  }
+  if (e != cudaSuccess)
+    return fail(LBM_ERR_CUDA, "step launch failed: %s", cudaGetErrorString(e));
+  if (s->pattern != LBM_AA)
+    s->cur ^= 1;
+  s->steps_done++;
+  s->launches++;
+  if (kind_out)
+    *kind_out = kind;
+  return LBM_OK;
+}
+
+extern "C" int lbm_run(lbm_solver *s, int steps)
+{
+  if (!s || steps < 0)
+    return fail(LBM_ERR_ARG, "lbm_run: bad arguments");
+  CUDA_TRY(cudaSetDevice(s->device));
+  for (int i = 0; i < steps; ++i) {
+    int rc = launch_one(s, NULL);
+    if (rc)
+      return rc;
+  }
+  return LBM_OK;
+}
+
+extern "C" int lbm_synchronize(lbm_solver *s)
+{
+  if (!s)
+    return fail(LBM_ERR_ARG, "lbm_synchronize: NULL solver");
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return LBM_OK;
+}
+
+extern "C" int lbm_run_timed(lbm_solver *s, int steps, double *ms)
+{
+  if (!s || steps < 0 || !ms)
+    return fail(LBM_ERR_ARG, "lbm_run_timed: bad arguments");
+  CUDA_TRY(cudaSetDevice(s->device));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  CUDA_TRY(cudaEventRecord(s->ev[0], s->stream));
+  int rc = lbm_run(s, steps);
+  if (rc)
+    return rc;
+  CUDA_TRY(cudaEventRecord(s->ev[1], s->stream));
+  CUDA_TRY(cudaEventSynchronize(s->ev[1]));
+  float t = 0.f;
+  CUDA_TRY(cudaEventElapsedTime(&t, s->ev[0], s->ev[1]));
+  *ms = t;
+  return LBM_OK;
+}
+
+extern "C" int lbm_time_launches(lbm_solver *s, int steps, double *ms_sum, int *count,
+    double *region_ms)
+{
+  if (!s || steps < 0 || !ms_sum || !count)
+    return fail(LBM_ERR_ARG, "lbm_time_launches: bad arguments");
+  CUDA_TRY(cudaSetDevice(s->device));
+  for (int k = 0; k < 4; ++k) {
+    ms_sum[k] = 0.0;
+    count[k] = 0;
+  }
+  std::vector<cudaEvent_t> ev(2 * (size_t)steps);
+  std::vector<int> kinds((size_t)steps);
+  for (auto &e : ev)
+    CUDA_TRY(cudaEventCreate(&e));
+  int rc = LBM_OK;
+  for (int i = 0; i < steps && !rc; ++i) {
+    cudaEventRecord(ev[2 * i], s->stream);
+    rc = launch_one(s, &kinds[i]);
+    cudaEventRecord(ev[2 * i + 1], s->stream);
+  }
+  cudaError_t e = cudaStreamSynchronize(s->stream);
+  for (int i = 0; i < steps && !rc && e == cudaSuccess; ++i) {
+    float t = 0.f;
+    e = cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]);
+    ms_sum[kinds[i]] += t;
+    count[kinds[i]] += 1;
+  }
+  if (region_ms) {
+    float t = 0.f;
+    if (steps > 0 && !rc && e == cudaSuccess)
+      e = cudaEventElapsedTime(&t, ev[0], ev[2 * (size_t)steps - 1]);
+    *region_ms = t;
+  }
+  for (auto &x : ev)
+    cudaEventDestroy(x);
+  if (rc)
+    return rc;
+  if (e != cudaSuccess)
+    return fail(LBM_ERR_CUDA, "lbm_time_launches: %s", cudaGetErrorString(e));
+  return LBM_OK;
+}
+
+template <class ST> static int moments_t(lbm_solver *s, double *q[4])
+{
+  dim3 grid, block;
+  cell_launch_shape(s->g, grid, block);
+  const size_t n = (size_t)s->nx * s->ny * s->nz;
+  const float inv = (float)(s->precision == LBM_F16 ? 1.0 / s->fp16_scale : 1.0);
+  for (int k = 0; k < 4; ++k) {
+    if (!q[k])
+      continue;
+    moments_kernel<ST><<<grid, block, 0, s->stream>>>(s->g, orientation(s), k,
+        (const typename ST::S *)state_ptr(s), s->mask, inv, s->staging);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(q[k], s->staging, sizeof(double) * n, cudaMemcpyDeviceToHost,
+        s->stream));
+  }
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return LBM_OK;
+}
+
+extern "C" int lbm_moments(lbm_solver *s, double *rho, double *ux, double *uy, double *uz)
+{
+  if (!s)
+    return fail(LBM_ERR_ARG, "lbm_moments: NULL solver");
+  CUDA_TRY(cudaSetDevice(s->device));
+  double *q[4] = { rho, ux, uy, uz };
+  switch (s->precision) {
+  case LBM_F64: return moments_t<StoreF64>(s, q);
+  case LBM_F32: return moments_t<StoreF32>(s, q);
+  default: return moments_t<StoreF16>(s, q);
+  }
+}
+
+template <class ST> static void mass_launch(lbm_solver *s, double *partial)
+{
+  const float inv = (float)(s->precision == LBM_F16 ? 1.0 / s->fp16_scale : 1.0);
+  mass_kernel<ST><<<kRedBlocks, kRedThreads, 0, s->stream>>>(s->g, orientation(s),
+      (const typename ST::S *)state_ptr(s), s->mask, inv, partial);
+}
+
+extern "C" int lbm_mass_momentum(lbm_solver *s, double out[4], long long *nonfinite)
+{
+  if (!s || !out)
+    return fail(LBM_ERR_ARG, "lbm_mass_momentum: NULL argument");
+  CUDA_TRY(cudaSetDevice(s->device));
+  if (s->precision == LBM_F64)
+    mass_launch<StoreF64>(s, s->red);
+  else if (s->precision == LBM_F32)
+    mass_launch<StoreF32>(s, s->red);
+  else
+    mass_launch<StoreF16>(s, s->red);
+  CUDA_TRY(cudaGetLastError());
+  double *fin = s->red + (size_t)kRedBlocks * kRedVals;
+  final_reduce_kernel<<<1, kRedThreads, 0, s->stream>>>(s->red, kRedBlocks, 0u, fin);
+  CUDA_TRY(cudaGetLastError());
+  double h[kRedVals];
+  CUDA_TRY(cudaMemcpyAsync(h, fin, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  for (int k = 0; k < 4; ++k)
+    out[k] = h[k];
+  long long bad = (long long)h[4];
+  if (nonfinite)
+    *nonfinite = bad;
+  if (bad)
+    return fail(LBM_ERR_NONFINITE, "state holds NaN/Inf in %lld fluid cells", bad);
+  return LBM_OK;
+}
+
+template <class SA, class SB> static void compare_launch(lbm_solver *a, lbm_solver *b)
+{
+  const float ia = (float)(a->precision == LBM_F16 ? 1.0 / a->fp16_scale : 1.0);
+  const float ib = (float)(b->precision == LBM_F16 ? 1.0 / b->fp16_scale : 1.0);
+  compare_kernel<SA, SB><<<kRedBlocks, kRedThreads, 0, a->stream>>>(a->g, b->g,
+      orientation(a), orientation(b), (const typename SA::S *)state_ptr(a),
+      (const typename SB::S *)state_ptr(b), a->mask, b->mask, ia, ib, a->red);
+}
+
+template <class SA> static void compare_b(lbm_solver *a, lbm_solver *b)
+{
+  if (b->precision == LBM_F64)
+    compare_launch<SA, StoreF64>(a, b);
+  else if (b->precision == LBM_F32)
+    compare_launch<SA, StoreF32>(a, b);
+  else
+    compare_launch<SA, StoreF16>(a, b);
+}
+
+extern "C" int lbm_compare(lbm_solver *a, lbm_solver *b, double out[6])
+{
+  if (!a || !b || !out)
+    return fail(LBM_ERR_ARG, "lbm_compare: NULL argument");
+  if (a->nx != b->nx || a->ny != b->ny || a->nz != b->nz || a->device != b->device)
+    return fail(LBM_ERR_ARG, "lbm_compare: solvers differ in size or device");
+  CUDA_TRY(cudaSetDevice(a->device));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  if (a->precision == LBM_F64)
+    compare_b<StoreF64>(a, b);
+  else if (a->precision == LBM_F32)
+    compare_b<StoreF32>(a, b);
+  else
+    compare_b<StoreF16>(a, b);
+  CUDA_TRY(cudaGetLastError());
+  double *fin = a->red + (size_t)kRedBlocks * kRedVals;
+  final_reduce_kernel<<<1, kRedThreads, 0, a->stream>>>(a->red, kRedBlocks, 0x30u, fin);
+  CUDA_TRY(cudaGetLastError());
+  double h[kRedVals];
+  CUDA_TRY(cudaMemcpyAsync(h, fin, sizeof(h), cudaMemcpyDeviceToHost, a->stream));
+  CUDA_TRY(cudaStreamSynchronize(a->stream));
+  for (int k = 0; k < 6; ++k)
+    out[k] = h[k];
+  return LBM_OK;
+}
+
+template <class ST> static void outlet_launch(lbm_solver *s)
+{
+  const float inv = (float)(s->precision == LBM_F16 ? 1.0 / s->fp16_scale : 1.0);
+  outlet_kernel<ST><<<kRedBlocks, kRedThreads, 0, s->stream>>>(s->g, orientation(s),
+      (const typename ST::S *)state_ptr(s), s->mask, inv, s->red);
+}
+
+extern "C" int lbm_objective(lbm_solver *s, double *j)
+{
+  if (!s || !j)
+    return fail(LBM_ERR_ARG, "lbm_objective: NULL argument");
+  CUDA_TRY(cudaSetDevice(s->device));
+  if (s->precision == LBM_F64)
+    outlet_launch<StoreF64>(s);
+  else if (s->precision == LBM_F32)
+    outlet_launch<StoreF32>(s);
+  else
+    outlet_launch<StoreF16>(s);
+  CUDA_TRY(cudaGetLastError());
+  double *fin = s->red + (size_t)kRedBlocks * kRedVals;
+  final_reduce_kernel<<<1, kRedThreads, 0, s->stream>>>(s->red, kRedBlocks, 0u, fin);
+  CUDA_TRY(cudaGetLastError());
+  double h[kRedVals];
+  CUDA_TRY(cudaMemcpyAsync(h, fin, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  *j = h[1] > 0 ? h[0] / h[1] : 0.0;
+  return LBM_OK;
+}
+
+extern "C" int lbm_pin_host(void *ptr, size_t bytes)
+{
+  if (!ptr || !bytes)
+    return fail(LBM_ERR_ARG, "lbm_pin_host: NULL or empty buffer");
+  CUDA_TRY(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
+  return LBM_OK;
+}
+
+extern "C" int lbm_unpin_host(void *ptr)
+{
+  if (!ptr)
+    return fail(LBM_ERR_ARG, "lbm_unpin_host: NULL buffer");
+  CUDA_TRY(cudaHostUnregister(ptr));
+  return LBM_OK;
+}
+
+extern "C" long long lbm_fluid_cells(const lbm_solver *s) { return s ? s->n_fluid : -1; }
+extern "C" long long lbm_steps_done(const lbm_solver *s) { return s ? s->steps_done : -1; }
+extern "C" size_t lbm_device_bytes(const lbm_solver *s) { return s ? s->dev_bytes : 0; }
+extern "C" long long lbm_launch_count(const lbm_solver *s) { return s ? s->launches : -1; }
+extern "C" double lbm_bytes_per_update(const lbm_solver *s)
+{
+  return s ? 2.0 * Q * (double)storage_size(s->precision) : 0.0;
+}

@@ -1,0 +1,288 @@
+"""Python binding of liblbmb200 (include/lbm_b200.h) over ctypes.
+
+The compute path is the CUDA library; this module only marshals arrays. If
+the library is missing, or no CUDA device is visible, solver construction
+raises - there is no CPU fallback.
+
+Array conventions (as the C ABI):
+  flags  int32[nz, ny, nx]         latticeIndex order of LBM-Bench, x fastest
+  f      float64[19, nx, ny, nz]   f[d, x, y, z], z fastest
+  cell arrays  [nx, ny, nz]
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblbmb200.so")
+
+PUSH, PULL, AA = 0, 1, 2
+F64, F32, F16 = 0, 1, 2
+PATTERNS = {"push": PUSH, "pull": PULL, "aa": AA}
+PRECISIONS = {"fp64": F64, "fp32": F32, "fp16": F16}
+Q = 19
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_fp = ctypes.POINTER(ctypes.c_float)
+_llp = ctypes.POINTER(ctypes.c_longlong)
+_vp = ctypes.c_void_p
+
+
+class LbmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+_lib = None
+
+# (name, restype, argtypes) of every exported function
+_SIGNATURES = [
+    ("lbm_create", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                  _ip, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_int]),
+    ("lbm_destroy", ctypes.c_int, [_vp]),
+    ("lbm_set_params", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_int]),
+    ("lbm_set_fp16_scale", ctypes.c_int, [_vp, ctypes.c_double]),
+    ("lbm_set_porosity", ctypes.c_int, [_vp, _fp, ctypes.c_double]),
+    ("lbm_set_state", ctypes.c_int, [_vp, _dp]),
+    ("lbm_get_state", ctypes.c_int, [_vp, _dp]),
+    ("lbm_run", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("lbm_synchronize", ctypes.c_int, [_vp]),
+    ("lbm_run_timed", ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    ("lbm_time_launches", ctypes.c_int, [_vp, ctypes.c_int, _dp, _ip, _dp]),
+    ("lbm_pin_host", ctypes.c_int, [_vp, ctypes.c_size_t]),
+    ("lbm_unpin_host", ctypes.c_int, [_vp]),
+    ("lbm_moments", ctypes.c_int, [_vp, _dp, _dp, _dp, _dp]),
+    ("lbm_mass_momentum", ctypes.c_int, [_vp, _dp, _llp]),
+    ("lbm_compare", ctypes.c_int, [_vp, _vp, _dp]),
+    ("lbm_objective", ctypes.c_int, [_vp, _dp]),
+    ("lbm_fluid_cells", ctypes.c_longlong, [_vp]),
+    ("lbm_steps_done", ctypes.c_longlong, [_vp]),
+    ("lbm_device_bytes", ctypes.c_size_t, [_vp]),
+    ("lbm_bytes_per_update", ctypes.c_double, [_vp]),
+    ("lbm_launch_count", ctypes.c_longlong, [_vp]),
+    ("lbm_last_error", ctypes.c_char_p, []),
+    ("lbm_device_count", ctypes.c_int, []),
+    ("lbm_geometry_create", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, _ip, _ip, _llp]),
+    ("lbm_porous_channel", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_ulonglong, _ip, _dp, _ip]),
+    ("lbm_perturbed_equilibrium", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip,
+                                                 ctypes.c_ulonglong, ctypes.c_double,
+                                                 ctypes.c_double, _dp]),
+]
+
+
+def lib() -> ctypes.CDLL:
+    """Loads liblbmb200.so (built by `make -C lbm-bench_b200`)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing: build it with `make -C {HERE}` (the CUDA library is "
+                "the only implementation; there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in _SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise LbmError(rc, lib().lbm_last_error().decode(errors="replace"))
+
+
+def _p(a: np.ndarray, kind):
+    return a.ctypes.data_as(kind)
+
+
+def device_count() -> int:
+    return lib().lbm_device_count()
+
+
+class Solver:
+    """One device lattice (include/lbm_b200.h lbm_create ... lbm_destroy)."""
+
+    def __init__(self, flags, periodic=(1, 0, 0), pattern=AA, precision=F64):
+        if isinstance(pattern, str):
+            pattern = PATTERNS[pattern]
+        if isinstance(precision, str):
+            precision = PRECISIONS[precision]
+        flags = np.ascontiguousarray(flags, dtype=np.int32)
+        nz, ny, nx = flags.shape
+        self.shape = (nx, ny, nz)
+        self.flags = flags
+        self.pattern, self.precision = pattern, precision
+        self.periodic = tuple(int(p) for p in periodic)
+        h = _vp()
+        _check(lib().lbm_create(ctypes.byref(h), nx, ny, nz, _p(flags, _ip), *self.periodic,
+                                pattern, precision))
+        self._h = h
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().lbm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- configuration -----------------------------------------------------
+    def set_params(self, omega=1.0, lam=1.0 / 12.0, xforce=1e-5, force_on=False):
+        _check(lib().lbm_set_params(self._h, omega, lam, xforce, int(force_on)))
+
+    def set_fp16_scale(self, scale: float):
+        _check(lib().lbm_set_fp16_scale(self._h, scale))
+
+    def set_porosity(self, porosity, alpha: float):
+        por = np.ascontiguousarray(porosity, dtype=np.float32)
+        _check(lib().lbm_set_porosity(self._h, _p(por, _fp), alpha))
+
+    # -- state -------------------------------------------------------------
+    def set_state(self, f):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        if f.shape != (Q,) + self.shape:
+            raise ValueError(f"state shape {f.shape} != {(Q,) + self.shape}")
+        _check(lib().lbm_set_state(self._h, _p(f, _dp)))
+
+    def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((Q,) + self.shape, dtype=np.float64)
+        if out.shape != (Q,) + self.shape or out.dtype != np.float64 or \
+                not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of the state's shape")
+        _check(lib().lbm_get_state(self._h, _p(out, _dp)))
+        return out
+
+    # -- stepping ----------------------------------------------------------
+    def run(self, steps: int):
+        _check(lib().lbm_run(self._h, int(steps)))
+
+    def synchronize(self):
+        _check(lib().lbm_synchronize(self._h))
+
+    def run_timed(self, steps: int) -> float:
+        ms = ctypes.c_double(0.0)
+        _check(lib().lbm_run_timed(self._h, int(steps), ctypes.byref(ms)))
+        return ms.value
+
+    def time_launches(self, steps: int):
+        """Runs `steps` steps with CUDA events around each launch. Returns
+        ({kind: (ms_sum, launches)} for kinds pull, push, aa_even, aa_odd,
+        region_ms from the first launch's start to the last one's end)."""
+        ms = np.zeros(4)
+        cnt = np.zeros(4, dtype=np.int32)
+        region = ctypes.c_double(0.0)
+        _check(lib().lbm_time_launches(self._h, int(steps), _p(ms, _dp), _p(cnt, _ip),
+                                       ctypes.byref(region)))
+        names = ("pull", "push", "aa_even", "aa_odd")
+        return ({names[k]: (float(ms[k]), int(cnt[k])) for k in range(4) if cnt[k]},
+                region.value)
+
+    # -- observables -------------------------------------------------------
+    def moments(self):
+        q = [np.empty(self.shape) for _ in range(4)]
+        _check(lib().lbm_moments(self._h, *[_p(a, _dp) for a in q]))
+        return q
+
+    def mass_momentum(self, check=True):
+        out = np.zeros(4)
+        bad = ctypes.c_longlong(0)
+        rc = lib().lbm_mass_momentum(self._h, _p(out, _dp), ctypes.byref(bad))
+        if check:
+            _check(rc)
+        return out, bad.value
+
+    def compare(self, other: "Solver"):
+        out = np.zeros(6)
+        _check(lib().lbm_compare(self._h, other._h, _p(out, _dp)))
+        return out
+
+    def objective(self) -> float:
+        j = ctypes.c_double(0.0)
+        _check(lib().lbm_objective(self._h, ctypes.byref(j)))
+        return j.value
+
+    @property
+    def fluid_cells(self) -> int:
+        return lib().lbm_fluid_cells(self._h)
+
+    @property
+    def steps_done(self) -> int:
+        return lib().lbm_steps_done(self._h)
+
+    @property
+    def device_bytes(self) -> int:
+        return lib().lbm_device_bytes(self._h)
+
+    @property
+    def bytes_per_update(self) -> float:
+        return lib().lbm_bytes_per_update(self._h)
+
+    @property
+    def launch_count(self) -> int:
+        return lib().lbm_launch_count(self._h)
+
+
+def pin(a: np.ndarray) -> None:
+    """Page-locks a numpy array's buffer (lbm_pin_host)."""
+    _check(lib().lbm_pin_host(a.ctypes.data, a.nbytes))
+
+
+def unpin(a: np.ndarray) -> None:
+    _check(lib().lbm_unpin_host(a.ctypes.data))
+
+
+# ---------------------------------------------------------------------------
+# host services
+# ---------------------------------------------------------------------------
+
+def geometry(kind: str, dims, periodic=(0, 0, 0)):
+    """LBM-Bench geometries; returns (flags, periodic, (fluid, obstacle))."""
+    nx, ny, nz = dims
+    flags = np.zeros((nz, ny, nx), dtype=np.int32)
+    per = np.array(periodic, dtype=np.int32)
+    counts = np.zeros(2, dtype=np.int64)
+    _check(lib().lbm_geometry_create(kind.encode(), nx, ny, nz, _p(per, _ip), _p(flags, _ip),
+                                     _p(counts, _llp)))
+    return flags, tuple(int(p) for p in per), (int(counts[0]), int(counts[1]))
+
+
+def porous_channel(dims, solid_fraction=0.2, rmin=4.0, rmax=8.0, seed=42):
+    """Channel plus seeded solid spheres; returns (flags, fraction, n_spheres)."""
+    nx, ny, nz = dims
+    flags = np.zeros((nz, ny, nx), dtype=np.int32)
+    frac = ctypes.c_double(0.0)
+    n = ctypes.c_int(0)
+    _check(lib().lbm_porous_channel(nx, ny, nz, solid_fraction, rmin, rmax, seed,
+                                    _p(flags, _ip), ctypes.byref(frac), ctypes.byref(n)))
+    return flags, frac.value, n.value
+
+
+def perturbed_equilibrium(flags, seed=1, amplitude=1e-4, rho=1.0):
+    flags = np.ascontiguousarray(flags, dtype=np.int32)
+    nz, ny, nx = flags.shape
+    f = np.empty((Q, nx, ny, nz))
+    _check(lib().lbm_perturbed_equilibrium(nx, ny, nz, _p(flags, _ip), seed, amplitude, rho,
+                                           _p(f, _dp)))
+    return f

@@ -1,0 +1,253 @@
+"""Test infrastructure only: ctypes bindings for the CPU oracle libraries.
+
+* ``liboracle.so`` - our C restatement of the D3Q19 TRT step (lbm_oracle.c).
+* ``_ref/libref_*.so`` - LBM-Bench's own sources compiled unmodified
+  (oracle/Makefile) behind ref_harness.c. Present only where the reference
+  tree was available at build time.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg import this module, and only as the checker / the timed CPU baseline.
+
+Array conventions (shared with the product's flat C API):
+  flags  int32[nz, ny, nx]   the reference's latticeIndex order, x fastest
+                             (src/lbm.h:108-111); 0 = obstacle, 1 = fluid.
+  f      float64[19, nx, ny, nz]  z fastest; f[d, x, y, z] is the population
+                             of direction d that cell (x,y,z) collides next.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+Q = 19
+
+# D3Q19 velocity set in the reference's direction order (src/lbm.c:20-29).
+CX = np.array([0, 0, 1, -1, 1, 1, -1, -1, 0, 0, 1, -1, 0, 0, 0, 0, -1, 1, 0])
+CY = np.array([1, -1, 0, 0, 1, -1, 1, -1, 0, 1, 0, 0, -1, 0, -1, 1, 0, 0, 0])
+CZ = np.array([0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, -1, -1, -1, -1, -1, 0])
+INV = np.array([int(np.flatnonzero((CX == -CX[d]) & (CY == -CY[d]) & (CZ == -CZ[d]))[0])
+                for d in range(19)])
+W = np.array([1 / 18] * 4 + [1 / 36] * 4 + [1 / 18] + [1 / 36] * 4 + [1 / 18] + [1 / 36] * 4
+             + [1 / 3])
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_fp = ctypes.POINTER(ctypes.c_float)
+
+
+def build(quiet: bool = True) -> None:
+    """Compiles liboracle.so (and oracle/_ref when the reference tree exists)."""
+    out = subprocess.run(["make", "-C", HERE, "all"], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
+
+
+def _ptr(a: np.ndarray, kind):
+    return a.ctypes.data_as(kind)
+
+
+class Oracle:
+    """Our C restatement (liboracle.so)."""
+
+    def __init__(self, path: str | None = None):
+        path = path or os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        L.orc_run.restype = ctypes.c_int
+        L.orc_run.argtypes = [ctypes.c_int] * 3 + [_ip] + [ctypes.c_int] * 3 + \
+            [ctypes.c_double] * 3 + [ctypes.c_int, ctypes.c_int, _dp, _dp]
+        L.orc_run_brinkman.restype = ctypes.c_int
+        L.orc_run_brinkman.argtypes = [ctypes.c_int] * 3 + [_ip] + [ctypes.c_int] * 3 + \
+            [ctypes.c_double] * 4 + [_fp, ctypes.c_int, _dp, _dp]
+        L.orc_objective.restype = ctypes.c_double
+        L.orc_objective.argtypes = [ctypes.c_int] * 3 + [_ip, _dp]
+        L.orc_adjoint_brinkman.restype = ctypes.c_int
+        L.orc_adjoint_brinkman.argtypes = [ctypes.c_int] * 3 + [_ip] + [ctypes.c_int] * 3 + \
+            [ctypes.c_double] * 4 + [_fp, ctypes.c_int, _dp, _dp, _dp]
+
+    def run(self, flags, periodic, f_in, steps, omega, lam, xforce, force_on=True):
+        nz, ny, nx = flags.shape
+        flags = np.ascontiguousarray(flags, dtype=np.int32)
+        f_in = np.ascontiguousarray(f_in, dtype=np.float64)
+        out = np.empty_like(f_in)
+        rc = self.lib.orc_run(nx, ny, nz, _ptr(flags, _ip), *[int(p) for p in periodic],
+                              omega, lam, xforce, int(force_on), steps, _ptr(f_in, _dp),
+                              _ptr(out, _dp))
+        if rc != 0:
+            raise RuntimeError("orc_run failed")
+        return out
+
+    def run_brinkman(self, flags, periodic, f_in, steps, omega, lam, xforce, alpha, porosity):
+        nz, ny, nx = flags.shape
+        flags = np.ascontiguousarray(flags, dtype=np.int32)
+        f_in = np.ascontiguousarray(f_in, dtype=np.float64)
+        por = np.ascontiguousarray(porosity, dtype=np.float32)
+        out = np.empty_like(f_in)
+        rc = self.lib.orc_run_brinkman(nx, ny, nz, _ptr(flags, _ip), *[int(p) for p in periodic],
+                                       omega, lam, xforce, alpha, _ptr(por, _fp), steps,
+                                       _ptr(f_in, _dp), _ptr(out, _dp))
+        if rc != 0:
+            raise RuntimeError("orc_run_brinkman failed")
+        return out
+
+    def objective(self, flags, f):
+        nz, ny, nx = flags.shape
+        flags = np.ascontiguousarray(flags, dtype=np.int32)
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        return self.lib.orc_objective(nx, ny, nz, _ptr(flags, _ip), _ptr(f, _dp))
+
+    def adjoint(self, flags, periodic, f_in, steps, omega, lam, xforce, alpha, porosity):
+        nz, ny, nx = flags.shape
+        flags = np.ascontiguousarray(flags, dtype=np.int32)
+        f_in = np.ascontiguousarray(f_in, dtype=np.float64)
+        por = np.ascontiguousarray(porosity, dtype=np.float32)
+        grad = np.zeros((nx, ny, nz), dtype=np.float64)
+        j = ctypes.c_double(0.0)
+        rc = self.lib.orc_adjoint_brinkman(nx, ny, nz, _ptr(flags, _ip),
+                                           *[int(p) for p in periodic], omega, lam, xforce,
+                                           alpha, _ptr(por, _fp), steps, _ptr(f_in, _dp),
+                                           _ptr(grad, _dp), ctypes.byref(j))
+        if rc != 0:
+            raise RuntimeError("orc_adjoint_brinkman failed")
+        return j.value, grad
+
+
+def ref_available(variant: str = "verify") -> bool:
+    return os.path.exists(os.path.join(REF_DIR, f"libref_{variant}.so"))
+
+
+class Reference:
+    """LBM-Bench's own kernels behind ref_harness.c (oracle/_ref)."""
+
+    def __init__(self, variant: str = "verify"):
+        path = os.path.join(REF_DIR, f"libref_{variant}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        L.ref_n_kernels.restype = ctypes.c_int
+        L.ref_kernel_name.restype = ctypes.c_char_p
+        L.ref_kernel_name.argtypes = [ctypes.c_int]
+        L.ref_max_threads.restype = ctypes.c_int
+        L.ref_geometry.restype = ctypes.c_int
+        L.ref_geometry.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   _ip, _ip, _ip, _ip]
+        L.ref_run.restype = ctypes.c_int
+        L.ref_run.argtypes = [ctypes.c_char_p] + [ctypes.c_int] * 3 + [_ip] + \
+            [ctypes.c_int] * 3 + [ctypes.c_double] * 2 + [ctypes.c_int, ctypes.c_int, _dp, _dp,
+                                                          _dp, _ip, _ip]
+        L.ref_verify.restype = ctypes.c_int
+        L.ref_verify.argtypes = [ctypes.c_int] * 3 + [_ip] + [ctypes.c_int] * 3 + \
+            [ctypes.c_double] * 2 + [_dp, _dp]
+        L.ref_initial_state.restype = ctypes.c_int
+        L.ref_initial_state.argtypes = [ctypes.c_char_p] + [ctypes.c_int] * 3 + [_ip] + \
+            [ctypes.c_int] * 3 + [ctypes.c_double, _dp]
+
+    def kernels(self):
+        return [self.lib.ref_kernel_name(i).decode() for i in range(self.lib.ref_n_kernels())]
+
+    def max_threads(self) -> int:
+        return self.lib.ref_max_threads()
+
+    def geometry(self, kind: str, dims, periodic=(0, 0, 0)):
+        nx, ny, nz = dims
+        flags = np.zeros((nz, ny, nx), dtype=np.int32)
+        pin = np.array(periodic, dtype=np.int32)
+        pout = np.zeros(3, dtype=np.int32)
+        counts = np.zeros(2, dtype=np.int32)
+        self.lib.ref_geometry(kind.encode(), nx, ny, nz, _ptr(pin, _ip), _ptr(flags, _ip),
+                              _ptr(pout, _ip), _ptr(counts, _ip))
+        return flags, tuple(int(p) for p in pout), (int(counts[0]), int(counts[1]))
+
+    def run(self, kernel, flags, periodic, f_in, steps, omega, xforce, inject=True,
+            readback=True):
+        """Returns (f_out or None, duration_s, final Iteration, nBounceBackPdfs).
+        duration_s is the reference kernel's own timing of its time loop."""
+        nz, ny, nx = flags.shape
+        flags = np.ascontiguousarray(flags, dtype=np.int32)
+        if f_in is None:
+            f_in = np.zeros((Q, nx, ny, nz))
+        f_in = np.ascontiguousarray(f_in, dtype=np.float64)
+        out = np.zeros_like(f_in) if readback else None
+        dur = ctypes.c_double(0.0)
+        it = ctypes.c_int(0)
+        nbb = ctypes.c_int(0)
+        rc = self.lib.ref_run(kernel.encode(), nx, ny, nz, _ptr(flags, _ip),
+                              *[int(p) for p in periodic], omega, xforce, steps, int(inject),
+                              _ptr(f_in, _dp), _ptr(out, _dp) if readback else None,
+                              ctypes.byref(dur),
+                              ctypes.byref(it), ctypes.byref(nbb))
+        if rc != 0:
+            raise KeyError(kernel)
+        return out, dur.value, it.value, nbb.value
+
+    def verify(self, flags, periodic, f, omega, xforce) -> float:
+        nz, ny, nx = flags.shape
+        flags = np.ascontiguousarray(flags, dtype=np.int32)
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        err = ctypes.c_double(0.0)
+        self.lib.ref_verify(nx, ny, nz, _ptr(flags, _ip), *[int(p) for p in periodic], omega,
+                            xforce, _ptr(f, _dp), ctypes.byref(err))
+        return err.value
+
+    def initial_state(self, kernel, flags, periodic, omega):
+        nz, ny, nx = flags.shape
+        flags = np.ascontiguousarray(flags, dtype=np.int32)
+        out = np.zeros((Q, nx, ny, nz))
+        self.lib.ref_initial_state(kernel.encode(), nx, ny, nz, _ptr(flags, _ip),
+                                   *[int(p) for p in periodic], omega, _ptr(out, _dp))
+        return out
+
+
+# ---------------------------------------------------------------------------
+# Seeded inputs shared by tests, fixtures and the CPU baseline
+# ---------------------------------------------------------------------------
+
+def equilibrium(rho, ux, uy, uz):
+    """Incompressible D3Q19 equilibrium matching the reference's collision
+    (src/kernel_pull_soa.c:128-198): w (rho - 1.5 u.u + 3 c.u + 4.5 (c.u)^2).
+    Shapes broadcast; returns float64[19, ...]."""
+    rho, ux, uy, uz = (np.asarray(a, dtype=np.float64) for a in (rho, ux, uy, uz))
+    usq = ux * ux + uy * uy + uz * uz
+    out = []
+    for d in range(Q):
+        cu = CX[d] * ux + CY[d] * uy + CZ[d] * uz
+        out.append(W[d] * (rho - 1.5 * usq + 3.0 * cu + 4.5 * cu * cu))
+    return np.stack(out)
+
+
+def perturbed_state(flags, seed, amp=1e-4, rho=1.0):
+    """Equilibrium at density rho with a seeded uniform velocity perturbation
+    u ~ U(-amp, amp)^3 per fluid cell; obstacle entries are zero."""
+    nz, ny, nx = flags.shape
+    rng = np.random.default_rng(seed)
+    u = rng.uniform(-amp, amp, size=(3, nx, ny, nz))
+    f = equilibrium(np.full((nx, ny, nz), rho), u[0], u[1], u[2])
+    fluid = np.transpose(flags, (2, 1, 0)) != 0
+    f[:, ~fluid] = 0.0
+    return f
+
+
+def fluid_mask(flags):
+    """bool[nx, ny, nz] of fluid cells."""
+    return np.transpose(flags, (2, 1, 0)) != 0
+
+
+def moments(f, flags):
+    """rho, ux, uy, uz (momentum, as the reference computes it) per cell,
+    zero on obstacles; each float64[nx, ny, nz]."""
+    rho = f.sum(axis=0)
+    ux = np.tensordot(CX.astype(np.float64), f, axes=(0, 0))
+    uy = np.tensordot(CY.astype(np.float64), f, axes=(0, 0))
+    uz = np.tensordot(CZ.astype(np.float64), f, axes=(0, 0))
+    m = fluid_mask(flags)
+    return [np.where(m, a, 0.0) for a in (rho, ux, uy, uz)]

@@ -1,0 +1,114 @@
+"""Host-side logic of liblbmb200 that needs no GPU: geometry generators, the
+seeded initial state, the exported C ABI, and the loud failure of the
+product path when no CUDA device is present."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import golden_io
+import lbmb200 as L
+import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+INCLUDE = os.path.join(ROOT, "include")
+
+GEOMS = [("channel", (12, 10, 14), (0, 0, 0)), ("box", (10, 9, 8), (1, 1, 0)),
+         ("box", (7, 8, 9), (0, 0, 0)), ("box", (7, 8, 9), (0, 1, 1)),
+         ("pipe", (9, 12, 11), (0, 0, 0)), ("pipe", (5, 20, 14), (0, 1, 0)),
+         ("blocks", (20, 18, 17), (0, 0, 0)), ("blocks-3", (13, 11, 9), (0, 0, 0)),
+         ("blocks-0", (17, 17, 17), (0, 0, 0)), ("fluid", (6, 7, 5), (0, 0, 0)),
+         ("CHANNEL", (4, 5, 6), (0, 0, 1))]
+
+
+@pytest.mark.parametrize("kind,dims,per", GEOMS)
+def test_geometry_matches_reference_rules(kind, dims, per):
+    flags, per_out, counts = L.geometry(kind, dims, per)
+    ref = golden_io.reference_geometry(kind, dims, per)
+    assert np.array_equal(flags != 0, ref != 0)
+    assert counts == (int((ref != 0).sum()), int((ref == 0).sum()))
+    if O.ref_available("verify"):
+        rflags, rper, rcounts = O.Reference("verify").geometry(kind, dims, per)
+        assert np.array_equal(flags != 0, rflags != 0)
+        assert per_out == rper
+        assert counts == rcounts
+
+
+def test_geometry_unknown_type_is_an_error():
+    with pytest.raises(L.LbmError):
+        L.geometry("sphere", (4, 4, 4))
+
+
+def test_porous_channel_is_seeded_and_reaches_fraction():
+    a, fa, na = L.porous_channel((48, 40, 36), 0.2, 3.0, 5.0, seed=3)
+    b, fb, nb = L.porous_channel((48, 40, 36), 0.2, 3.0, 5.0, seed=3)
+    c, _, _ = L.porous_channel((48, 40, 36), 0.2, 3.0, 5.0, seed=4)
+    assert np.array_equal(a, b) and fa == fb and na == nb
+    assert not np.array_equal(a, c)
+    assert 0.2 <= fa < 0.2 + 0.05
+    assert fa == pytest.approx((a == 0).mean())
+    # channel walls are there, x is periodic (no x walls)
+    assert np.all(a[:, 0, :] == 0) and np.all(a[:, -1, :] == 0)
+    assert np.all(a[0, :, :] == 0) and np.all(a[-1, :, :] == 0)
+    assert (a[:, :, 0] != 0).any()
+
+
+def test_porous_channel_spheres_wrap_in_x():
+    flags, _, n = L.porous_channel((16, 40, 40), 0.3, 6.0, 7.0, seed=11)
+    # with radius >= 6 on a 16-long periodic axis, some sphere crosses x=0
+    interior = flags[1:-1, 1:-1, :] == 0
+    assert (interior[:, :, 0] & interior[:, :, -1]).any()
+
+
+def test_porous_channel_bad_args():
+    with pytest.raises(L.LbmError):
+        L.porous_channel((8, 8, 8), 0.99, 2, 3)
+    with pytest.raises(L.LbmError):
+        L.porous_channel((8, 8, 8), 0.2, 3, 2)
+
+
+def test_perturbed_equilibrium_moments():
+    flags, _, _ = L.geometry("channel", (10, 9, 8))
+    f = L.perturbed_equilibrium(flags, seed=5, amplitude=1e-3, rho=1.0)
+    g = L.perturbed_equilibrium(flags, seed=5, amplitude=1e-3, rho=1.0)
+    assert np.array_equal(f, g)
+    rho, ux, uy, uz = O.moments(f, flags)
+    m = O.fluid_mask(flags)
+    assert np.allclose(rho[m], 1.0, atol=1e-15)
+    for u in (ux, uy, uz):
+        assert np.abs(u[m]).max() <= 1e-3 * (1 + 1e-12)
+        assert np.abs(u[m]).max() > 5e-4
+    assert np.all(f[:, ~m] == 0.0)
+    # equals the oracle module's equilibrium for the same velocities
+    assert np.allclose(f[:, m], O.equilibrium(rho[m], ux[m], uy[m], uz[m]), atol=1e-17)
+
+
+def _declared_functions():
+    names = []
+    for fn in os.listdir(INCLUDE):
+        if not fn.endswith(".h"):
+            continue
+        src = open(os.path.join(INCLUDE, fn)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names += re.findall(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b([A-Za-z_]\w*)\s*\(",
+                            src, flags=re.M)
+    return sorted(set(n for n in names if n not in ("defined",)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = L.lib()
+    names = _declared_functions()
+    assert "lbm_create" in names and "lbm_run" in names
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+@pytest.mark.skipif(L.device_count() > 0, reason="a CUDA device is present")
+def test_product_path_fails_loudly_without_gpu():
+    flags, per, _ = L.geometry("channel", (8, 8, 8))
+    with pytest.raises(L.LbmError) as e:
+        L.Solver(flags, per)
+    assert e.value.code == -6
+    assert "no CPU path" in str(e.value)
