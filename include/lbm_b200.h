@@ -123,6 +123,29 @@ int lbm_moments(lbm_solver *s, double *rho, double *ux, double *uy, double *uz);
  * kernelDensity (src/lbm.c:928-947) is out[0] / lbm_fluid_cells(). */
 int lbm_mass_momentum(lbm_solver *s, double out[4], long long *nonfinite);
 
+/* No counterpart in the reference. Same totals as lbm_mass_momentum, for a
+ * caller that holds the populations itself and must not allocate device
+ * memory: code running while a CUDA graph is captured (cudaMalloc is refused
+ * then), plug-ins whose host application's allocator owns the device memory,
+ * and loops that cannot afford cudaMalloc's device-wide synchronisation.
+ * This call allocates nothing: its scratch is a fixed array inside the
+ * library that every GPU loading the library holds until exit.
+ *   f      device pointer, double[19*nx*ny*nz] in the f[d][x][y][z] layout
+ *   flags  device pointer, int[nx*ny*nz] in latticeIndex order, 0 = obstacle
+ *   out    host double[4]: mass, momentum x, y, z over fluid cells (FP64)
+ *   nonfinite  host, may be NULL: fluid cells holding NaN/Inf (if non-zero
+ *          the call returns LBM_ERR_NONFINITE after filling out)
+ *   stream cudaStream_t as void* (NULL = default stream); the call waits
+ *          for its own work on that stream.
+ * Limit: nx <= LBM_NOALLOC_MAX_PLANES (one scratch row per x-plane); larger
+ * boxes are rejected with LBM_ERR_ARG. The first call on each device looks
+ * up the scratch's device address; make it before any stream capture.
+ * Calls share the scratch: calls whose work overlaps on the GPU race, so
+ * serialise them. */
+#define LBM_NOALLOC_MAX_PLANES 8192
+int lbm_mass_momentum_noalloc(const double *f, const int *flags, int nx, int ny, int nz,
+    double out[4], long long *nonfinite, void *stream);
+
 /* Difference of two solvers over the same geometry (the first is compared
  * against the second, e.g. an FP16 run against an FP64 run):
  * out[0] = sum |u_a - u_b|^2, out[1] = sum |u_b|^2,

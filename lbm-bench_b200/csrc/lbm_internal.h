@@ -19,6 +19,9 @@ cudaError_t launch_step_f32(int kind, bool force, bool brink, const StepArgs<Sto
 cudaError_t launch_step_f16(int kind, bool force, bool brink, const StepArgs<StoreF16> &a,
     dim3 grid, dim3 block, cudaStream_t st);
 
+// Records the message returned by lbm_last_error() and returns `code`.
+int record_error(int code, const char *fmt, ...);
+
 // Block/grid shape of the per-cell kernels: z across lanes, then y, one
 // x-plane per grid.z.
 inline void cell_launch_shape(const Grid &g, dim3 &grid, dim3 &block)

@@ -70,6 +70,15 @@ struct lbm_solver {
 
 extern "C" const char *lbm_last_error(void) { return g_err; }
 
+int lbm::record_error(int code, const char *fmt, ...)
+{
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
 extern "C" int lbm_device_count(void)
 {
   int n = 0;

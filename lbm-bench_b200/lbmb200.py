@@ -61,6 +61,8 @@ _SIGNATURES = [
     ("lbm_moments", ctypes.c_int, [_vp, _dp, _dp, _dp, _dp]),
     ("lbm_mass_momentum", ctypes.c_int, [_vp, _dp, _llp]),
     ("lbm_compare", ctypes.c_int, [_vp, _vp, _dp]),
+    ("lbm_mass_momentum_noalloc", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_int, _dp, _llp, _vp]),
     ("lbm_objective", ctypes.c_int, [_vp, _dp]),
     ("lbm_fluid_cells", ctypes.c_longlong, [_vp]),
     ("lbm_steps_done", ctypes.c_longlong, [_vp]),
