@@ -9,18 +9,16 @@
 //                  src/kernel_pull_soa.c:203-204, src/kernel_aa_soa.c:154-155,277-278
 //   body force     src/lbm.c:902-922, applied after every step under -DVERIFICATION
 //
-// Device layout ("plane layout"): population d of cell (x,y,z) lives at
-//   f[d * plane + (x * ny + y) * pz + z]
-// z is the unit-stride axis, as in the reference's indexSoA
-// (src/lbm.h:113-116), but without ghost cells: periodic neighbours are
-// addressed by wrapping and bounce-back links never leave the cell. pz is
-// nz rounded up so that every z-row starts on a 32-byte sector; plane is
-// nx * ny * pz rounded up to 256 bytes.
+// Device layout ("plane layout"): population d of cell index c lives at
+//   f[d * plane + c]
+// with the cell index of struct Grid below: z is the unit-stride axis, as
+// in the reference's indexSoA (src/lbm.h:113-116); periodic neighbours are
+// addressed by wrapping instead of through ghost copies.
 //
 // Link mask: one 32-bit word per cell. Bit d (0..18) is set when the
-// neighbour x + c_d is an obstacle or lies outside a non-periodic axis, so
-// the population leaving along d bounces back. Bit 31 marks an obstacle
-// cell, which is never computed.
+// neighbour x + c_d is an obstacle, so the population leaving along d
+// bounces back. Bit 31 marks a wall cell (obstacle, frame or row padding),
+// which is never computed.
 #pragma once
 
 #include <cuda_fp16.h>
@@ -69,9 +67,9 @@ __host__ __device__ constexpr int wclass(int d)
 // Propagation patterns and the state orientations they leave behind.
 enum Pattern { kPull = 0, kPush = 1, kAA = 2 };
 enum Orientation {
-  kNatural = 0, // f_d(x) at (d, x): push state, AA after an odd step, initial AA state
-  kPullState = 1, // f_d(x) at (d, x - c_d); at (inv d, x) if x - c_d bounces
-  kAAEven = 2     // f_d(x) at (inv d, x - c_d); at (d, x) if x - c_d bounces
+  kNatural = 0,   // f_d(x) at (d, x): push state, AA after an odd step, initial AA state
+  kPullState = 1, // f_d(x) at (d, x - c_d); at (inv d, x) if x - c_d is a wall
+  kAAEven = 2     // f_d(x) at (inv d, x - c_d); at (d, x) if x - c_d is a wall
 };
 enum Kind { kPullStep = 0, kPushStep = 1, kAAEvenStep = 2, kAAOddStep = 3 };
 
@@ -82,6 +80,8 @@ struct StoreF64 {
   using S = double;
   using V = double;
   static constexpr bool kShifted = false;
+  __device__ static V decode(S s, V) { return s; }
+  __device__ static S encode(V v, V) { return v; }
   __device__ static V load(const S *p, int, V) { return *p; }
   __device__ static void store(S *p, V v, V) { *p = v; }
 };
@@ -89,6 +89,8 @@ struct StoreF32 {
   using S = float;
   using V = float;
   static constexpr bool kShifted = true;
+  __device__ static V decode(S s, V) { return s; }
+  __device__ static S encode(V v, V) { return v; }
   __device__ static V load(const S *p, int, V) { return *p; }
   __device__ static void store(S *p, V v, V) { *p = v; }
 };
@@ -97,6 +99,8 @@ struct StoreF16 {
   using S = __half;
   using V = float;
   static constexpr bool kShifted = true;
+  __device__ static V decode(S s, V inv_scale) { return __half2float(s) * inv_scale; }
+  __device__ static S encode(V v, V scale) { return __float2half_rn(v * scale); }
   __device__ static V load(const S *p, int, V inv_scale) { return __half2float(*p) * inv_scale; }
   __device__ static void store(S *p, V v, V scale) { *p = __float2half_rn(v * scale); }
 };
@@ -160,63 +164,90 @@ __device__ __forceinline__ void collide(const V (&f)[Q], V (&o)[Q], const Consts
 }
 
 // Geometry of the device lattice, passed by value to every kernel.
+// Cell (x, y, z), 0 <= x < nx etc., lives at cell = (x * ny + y) * pz + z;
+// rows start on 32-byte sectors (pz rounds nz up) and the plane is rounded
+// to 256 bytes. Periodic axes wrap. On a non-periodic axis every face cell
+// is a wall: the reference's geometries put obstacle cells there
+// (src/lbm.c:104-129), and where a caller's flags leave fluid on such a
+// face the host embeds the box in a one-cell solid frame, so a fluid cell's
+// neighbour always exists and a bounced population always has a wall slot
+// to sit in (as in the reference's obstacle and ghost slots,
+// src/lbm.c:532-566).
 struct Grid {
-  int nx, ny, nz, pz;
+  int nx, ny, nz;  // device extent (the caller's box plus frames)
+  int pz;          // z pitch of a row, elements
+  int per;         // periodic axes: bit 0 x, bit 1 y, bit 2 z
   long long plane; // elements per direction plane
 };
 
-// Cell coordinates -> cell index in the plane layout.
-__device__ __forceinline__ long long cell_index(const Grid &g, int x, int y, int z)
+// Caller's box inside the device box: offsets and extent.
+struct UserBox {
+  int ox, oy, oz;
+  int nx, ny, nz;
+};
+
+// Cell index of device coordinates (below 2^32, checked at creation).
+__device__ __forceinline__ uint32_t cell_index(const Grid &g, int x, int y, int z)
 {
-  return ((long long)x * g.ny + y) * g.pz + z;
+  return ((uint32_t)x * (uint32_t)g.ny + (uint32_t)y) * (uint32_t)g.pz + (uint32_t)z;
 }
 
-// The 3x3x3 wrapped neighbourhood of a cell, from which each direction's
-// neighbour index is one add. Wrapping happens on every axis: a link that
-// leaves a non-periodic axis is flagged in the mask and never dereferenced.
-struct Nbhd {
-  long long row[3][3]; // row[cx+1][cy+1] = (x' * ny + y') * pz
-  int zz[3];           // z', for cz = -1, 0, 1
-  __device__ __forceinline__ long long at(int d) const
+// Neighbour offsets of one cell, in cells, as 32-bit unsigned values:
+// cell + at(d) (mod 2^32) is the neighbour x + c_d, wrapped across periodic
+// axes. Only meaningful for fluid cells (which never sit on a non-periodic
+// face). The x and y parts are uniform across a warp (a warp never spans
+// two (x, y) rows); the z parts differ only at the ends of a row.
+struct Offs {
+  uint32_t xm, xp, ym, yp, zm, zp;
+  __device__ __forceinline__ uint32_t at(int d) const
   {
-    return row[cx(d) + 1][cy(d) + 1] + zz[cz(d) + 1];
+    uint32_t o = 0u;
+    if (cx(d) < 0)
+      o += xm;
+    else if (cx(d) > 0)
+      o += xp;
+    if (cy(d) < 0)
+      o += ym;
+    else if (cy(d) > 0)
+      o += yp;
+    if (cz(d) < 0)
+      o += zm;
+    else if (cz(d) > 0)
+      o += zp;
+    return o;
   }
 };
 
-__device__ __forceinline__ Nbhd make_nbhd(const Grid &g, int x, int y, int z)
+__device__ __forceinline__ Offs make_offs(const Grid &g, int x, int y, int z)
 {
-  Nbhd n;
-  const int xs[3] = { x == 0 ? g.nx - 1 : x - 1, x, x == g.nx - 1 ? 0 : x + 1 };
-  const int ys[3] = { y == 0 ? g.ny - 1 : y - 1, y, y == g.ny - 1 ? 0 : y + 1 };
-  n.zz[0] = z == 0 ? g.nz - 1 : z - 1;
-  n.zz[1] = z;
-  n.zz[2] = z == g.nz - 1 ? 0 : z + 1;
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int b = 0; b < 3; ++b)
-      n.row[a][b] = ((long long)xs[a] * g.ny + ys[b]) * g.pz;
-  return n;
+  const uint32_t sy = (uint32_t)g.pz, sx = (uint32_t)g.ny * (uint32_t)g.pz;
+  const bool px = g.per & 1, py = (g.per >> 1) & 1, pzz = (g.per >> 2) & 1;
+  Offs o;
+  o.xm = (px && x == 0) ? (uint32_t)(g.nx - 1) * sx : 0u - sx;
+  o.xp = (px && x == g.nx - 1) ? 0u - (uint32_t)(g.nx - 1) * sx : sx;
+  o.ym = (py && y == 0) ? (uint32_t)(g.ny - 1) * sy : 0u - sy;
+  o.yp = (py && y == g.ny - 1) ? 0u - (uint32_t)(g.ny - 1) * sy : sy;
+  o.zm = (pzz && z == 0) ? (uint32_t)(g.nz - 1) : 0u - 1u;
+  o.zp = (pzz && z == g.nz - 1) ? 0u - (uint32_t)(g.nz - 1) : 1u;
+  return o;
 }
 
-// Neighbour x - c_d is the neighbour x + c_{inv d}.
-__device__ __forceinline__ long long behind(const Nbhd &n, int d) { return n.at(inv(d)); }
-
-// Where f_d(x) of fluid cell x lives in a state of orientation `o`:
-// plane index and cell index.
-__device__ __forceinline__ void state_slot(int o, int d, uint32_t mask, long long cell,
-    const Nbhd &n, int &plane_out, long long &cell_out)
+// Where f_d(x) of a fluid cell lives in a state of orientation `o` (plane
+// index, cell index). A population that bounced off the wall x - c_d is kept
+// in a slot of the cell itself that no neighbour uses.
+__device__ __forceinline__ void state_slot(int o, int d, uint32_t mask, uint32_t cell,
+    const Offs &n, int &plane_out, uint32_t &cell_out)
 {
-  const bool bounced = (mask >> inv(d)) & 1u; // x - c_d is a wall
+  const bool back = (mask >> inv(d)) & 1u; // x - c_d is a wall
   if (o == kNatural) {
     plane_out = d;
     cell_out = cell;
   } else if (o == kPullState) {
-    plane_out = bounced ? inv(d) : d;
-    cell_out = bounced ? cell : behind(n, d);
+    plane_out = back ? inv(d) : d;
+    cell_out = back ? cell : cell + n.at(inv(d));
   } else {
-    plane_out = bounced ? d : inv(d);
-    cell_out = bounced ? cell : behind(n, d);
+    plane_out = back ? d : inv(d);
+    cell_out = back ? cell : cell + n.at(inv(d));
   }
 }
 

@@ -5,19 +5,21 @@
 #include <cuda_runtime.h>
 
 #include "lbm_step.cuh"
+#include "lbm_step_x2.cuh"
 
 namespace lbm {
 
 enum Precision { kF64 = 0, kF32 = 1, kF16 = 2 };
 
-// Step launchers, one per storage type (lbm_step_f64.cu is compiled with
-// --fmad=false for bit-exact reference arithmetic; lbm_step_lp.cu is not).
+// Step launchers: FP64 one cell per thread (lbm_step_f64.cu, compiled with
+// --fmad=false for bit-exact reference arithmetic), FP32/FP16 storage two
+// cells per thread (lbm_step_lp.cu).
 cudaError_t launch_step_f64(int kind, bool force, bool brink, const StepArgs<StoreF64> &a,
     dim3 grid, dim3 block, cudaStream_t st);
-cudaError_t launch_step_f32(int kind, bool force, bool brink, const StepArgs<StoreF32> &a,
-    dim3 grid, dim3 block, cudaStream_t st);
-cudaError_t launch_step_f16(int kind, bool force, bool brink, const StepArgs<StoreF16> &a,
-    dim3 grid, dim3 block, cudaStream_t st);
+cudaError_t launch_step_x2_f32(int kind, bool force, bool brink, const StepArgs2<StoreF32> &a,
+    cudaStream_t st);
+cudaError_t launch_step_x2_f16(int kind, bool force, bool brink, const StepArgs2<StoreF16> &a,
+    cudaStream_t st);
 
 // Records the message returned by lbm_last_error() and returns `code`.
 int record_error(int code, const char *fmt, ...);

@@ -44,10 +44,11 @@ static int fail(int code, const char *fmt, ...)
   } while (0)
 
 struct lbm_solver {
-  int nx, ny, nz;
+  int nx, ny, nz; // caller's box
   int periodic[3];
   int pattern, precision;
-  Grid g;
+  Grid g;     // device box (caller's box plus solid frames where needed)
+  UserBox ub; // caller's box inside the device box
   int device;
   cudaStream_t stream;
   cudaEvent_t ev[2];
@@ -66,6 +67,7 @@ struct lbm_solver {
   double fp16_scale;
   long long launches;
   size_t dev_bytes;
+  int no_shuffle; // reduced precision: never use the shuffle-aligned kernels
 };
 
 extern "C" const char *lbm_last_error(void) { return g_err; }
@@ -133,24 +135,49 @@ template <typename V> static Consts<V> make_consts(const lbm_solver *s)
   return c;
 }
 
+// Constants of the two-cell reduced-precision kernels, in storage units
+// G = S g (S = 1 for FP32): the linear terms are unchanged, the quadratic
+// ones (4.5 w ui^2 and 1.5 |u|^2) carry 1/S, forces carry S.
+static Consts2 make_consts2(const lbm_solver *s)
+{
+  const double S = s->precision == LBM_F16 ? s->fp16_scale : 1.0;
+  const double w1 = 1.0 / 18.0, w2 = 1.0 / 36.0;
+  Consts2 c;
+  c.oE    = (float)s->omega;
+  c.oO    = (float)(1.0 / (0.5 + s->lambda / (1.0 / s->omega - 0.5)));
+  c.w0    = (float)(1.0 / 3.0);
+  c.w1    = (float)w1;
+  c.w2    = (float)w2;
+  c.w1X3  = (float)(w1 * 3.0);
+  c.w2X3  = (float)(w2 * 3.0);
+  c.w1NHq = (float)(w1 * 4.5 / S);
+  c.w2NHq = (float)(w2 * 4.5 / S);
+  c.c15q  = (float)(1.5 / S);
+  for (int d = 0; d < Q; ++d)
+    c.force[d] = (float)(S * 3.0 * weight(d) * (double)cx(d) * s->xforce);
+  c.alpha = (float)s->alpha;
+  return c;
+}
+
 // ---------------------------------------------------------------------------
 // Auxiliary kernels
 // ---------------------------------------------------------------------------
 
-// One thread per cell of the padded box (z < pz); cells with z >= nz are
-// padding and are marked solid.
-__global__ void mask_kernel(Grid g, int px, int py, int pz, const uint8_t *fluid, uint32_t *mask)
+// One thread per device cell (z < pz): fluid cells get their link mask,
+// every other cell (obstacle, frame, row padding) the wall bit.
+__global__ void mask_kernel(Grid g, const uint8_t *fluid, uint32_t *mask)
 {
   const int z = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int x = blockIdx.z;
   if (z >= g.pz || y >= g.ny)
     return;
-  const long long cell = cell_index(g, x, y, z);
+  const uint32_t cell = cell_index(g, x, y, z);
   if (z >= g.nz || !fluid[cell]) {
     mask[cell] = kSolidBit;
     return;
   }
+  const bool px = g.per & 1, py = (g.per >> 1) & 1, pz = (g.per >> 2) & 1;
   uint32_t m = 0;
 #pragma unroll
   for (int d = 0; d < Q; ++d) {
@@ -182,31 +209,33 @@ __global__ void mask_kernel(Grid g, int px, int py, int pz, const uint8_t *fluid
   mask[cell] = m;
 }
 
-__device__ __forceinline__ long long dense_index(const Grid &g, int x, int y, int z)
+// Index of caller cell (x, y, z) in the caller's dense arrays.
+__device__ __forceinline__ long long dense_index(const UserBox &u, int x, int y, int z)
 {
-  return ((long long)x * g.ny + y) * g.nz + z;
+  return ((long long)x * u.ny + y) * u.nz + z;
 }
 
 // Dense plane d (caller layout) -> device state in orientation `orient`.
 template <class ST>
-__global__ void pack_plane_kernel(Grid g, int d, int orient, const double *__restrict__ dense,
-    typename ST::S *state, const uint32_t *__restrict__ mask, float scale, double wd)
+__global__ void pack_plane_kernel(Grid g, UserBox u, int d, int orient,
+    const double *__restrict__ dense, typename ST::S *state, const uint32_t *__restrict__ mask,
+    float scale, double wd)
 {
   using V = typename ST::V;
   const int z = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int x = blockIdx.z;
-  if (z >= g.nz || y >= g.ny)
+  if (z >= u.nz || y >= u.ny)
     return;
-  const long long cell = cell_index(g, x, y, z);
+  const uint32_t cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
   const uint32_t m = mask[cell];
   if (m & kSolidBit)
     return;
-  Nbhd nb = make_nbhd(g, x, y, z);
+  const Offs nb = make_offs(g, x + u.ox, y + u.oy, z + u.oz);
   int p;
-  long long c;
+  uint32_t c;
   state_slot(orient, d, m, cell, nb, p, c);
-  double v = dense[dense_index(g, x, y, z)];
+  double v = dense[dense_index(u, x, y, z)];
   if (ST::kShifted)
     v -= wd;
   ST::store(state + (long long)p * g.plane + c, (V)v, (V)scale);
@@ -214,36 +243,37 @@ __global__ void pack_plane_kernel(Grid g, int d, int orient, const double *__res
 
 // Device state -> dense plane d (caller layout); obstacles get 0.
 template <class ST>
-__global__ void unpack_plane_kernel(Grid g, int d, int orient, double *__restrict__ dense,
-    const typename ST::S *state, const uint32_t *__restrict__ mask, float inv_scale, double wd)
+__global__ void unpack_plane_kernel(Grid g, UserBox u, int d, int orient,
+    double *__restrict__ dense, const typename ST::S *state, const uint32_t *__restrict__ mask,
+    float inv_scale, double wd)
 {
   using V = typename ST::V;
   const int z = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int x = blockIdx.z;
-  if (z >= g.nz || y >= g.ny)
+  if (z >= u.nz || y >= u.ny)
     return;
-  const long long cell = cell_index(g, x, y, z);
+  const uint32_t cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
   const uint32_t m = mask[cell];
   if (m & kSolidBit) {
-    dense[dense_index(g, x, y, z)] = 0.0;
+    dense[dense_index(u, x, y, z)] = 0.0;
     return;
   }
-  Nbhd nb = make_nbhd(g, x, y, z);
+  const Offs nb = make_offs(g, x + u.ox, y + u.oy, z + u.oz);
   int p;
-  long long c;
+  uint32_t c;
   state_slot(orient, d, m, cell, nb, p, c);
   double v = (double)ST::load(state + (long long)p * g.plane + c, d, (V)inv_scale);
   if (ST::kShifted)
     v += wd;
-  dense[dense_index(g, x, y, z)] = v;
+  dense[dense_index(u, x, y, z)] = v;
 }
 
 // Density and momentum of one fluid cell in FP64. For shifted storage the
 // density is 1 + sum g (the shift sums to 1, its first moment to 0).
 template <class ST>
 __device__ __forceinline__ void cell_moments(const Grid &g, const typename ST::S *state,
-    int orient, uint32_t m, long long cell, const Nbhd &nb, float inv_scale, double &rho,
+    int orient, uint32_t m, uint32_t cell, const Offs &nb, float inv_scale, double &rho,
     double &jx, double &jy, double &jz, bool &finite)
 {
   using V = typename ST::V;
@@ -253,7 +283,7 @@ __device__ __forceinline__ void cell_moments(const Grid &g, const typename ST::S
 #pragma unroll
   for (int d = 0; d < Q; ++d) {
     int p;
-    long long c;
+    uint32_t c;
     state_slot(orient, d, m, cell, nb, p, c);
     const double v = (double)ST::load(state + (long long)p * g.plane + c, d, (V)inv_scale);
     finite = finite && isfinite(v);
@@ -266,25 +296,25 @@ __device__ __forceinline__ void cell_moments(const Grid &g, const typename ST::S
 
 // quantity: 0 rho, 1 ux, 2 uy, 3 uz (momentum) -> dense cell array
 template <class ST>
-__global__ void moments_kernel(Grid g, int orient, int quantity, const typename ST::S *state,
-    const uint32_t *__restrict__ mask, float inv_scale, double *out)
+__global__ void moments_kernel(Grid g, UserBox u, int orient, int quantity,
+    const typename ST::S *state, const uint32_t *__restrict__ mask, float inv_scale, double *out)
 {
   const int z = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int x = blockIdx.z;
-  if (z >= g.nz || y >= g.ny)
+  if (z >= u.nz || y >= u.ny)
     return;
-  const long long cell = cell_index(g, x, y, z);
+  const uint32_t cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
   const uint32_t m = mask[cell];
   double r = 0.0;
   if (!(m & kSolidBit)) {
-    Nbhd nb = make_nbhd(g, x, y, z);
+    const Offs nb = make_offs(g, x + u.ox, y + u.oy, z + u.oz);
     double rho, jx, jy, jz;
     bool fin;
     cell_moments<ST>(g, state, orient, m, cell, nb, inv_scale, rho, jx, jy, jz, fin);
     r = quantity == 0 ? rho : quantity == 1 ? jx : quantity == 2 ? jy : jz;
   }
-  out[dense_index(g, x, y, z)] = r;
+  out[dense_index(u, x, y, z)] = r;
 }
 
 constexpr int kRedThreads = 256;
@@ -327,11 +357,11 @@ __global__ void __launch_bounds__(kRedThreads) mass_kernel(Grid g, int orient,
     const long long r = i / g.nz;
     const int y = (int)(r % g.ny);
     const int x = (int)(r / g.ny);
-    const long long cell = cell_index(g, x, y, z);
+    const uint32_t cell = cell_index(g, x, y, z);
     const uint32_t m = mask[cell];
     if (m & kSolidBit)
       continue;
-    Nbhd nb = make_nbhd(g, x, y, z);
+    const Offs nb = make_offs(g, x, y, z);
     double rho, jx, jy, jz;
     bool fin;
     cell_moments<ST>(g, state, orient, m, cell, nb, inv_scale, rho, jx, jy, jz, fin);
@@ -373,11 +403,11 @@ __global__ void __launch_bounds__(kRedThreads) compare_kernel(Grid ga, Grid gb, 
     const long long r = i / ga.nz;
     const int y = (int)(r % ga.ny);
     const int x = (int)(r / ga.ny);
-    const long long ca = cell_index(ga, x, y, z), cb = cell_index(gb, x, y, z);
+    const uint32_t ca = cell_index(ga, x, y, z), cb = cell_index(gb, x, y, z);
     const uint32_t ma = mask_a[ca], mb = mask_b[cb];
     if ((ma & kSolidBit) || (mb & kSolidBit))
       continue;
-    Nbhd na = make_nbhd(ga, x, y, z), nbb = make_nbhd(gb, x, y, z);
+    const Offs na = make_offs(ga, x, y, z), nbb = make_offs(gb, x, y, z);
     double ra, xa, ya, za, rb, xb, yb, zb;
     bool fa, fb;
     cell_moments<SA>(ga, sa, oa, ma, ca, na, inv_a, ra, xa, ya, za, fa);
@@ -396,22 +426,21 @@ __global__ void __launch_bounds__(kRedThreads) compare_kernel(Grid ga, Grid gb, 
 
 // Sum of the x momentum and fluid count over the plane x = nx-1.
 template <class ST>
-__global__ void __launch_bounds__(kRedThreads) outlet_kernel(Grid g, int orient,
+__global__ void __launch_bounds__(kRedThreads) outlet_kernel(Grid g, int x, int orient,
     const typename ST::S *state, const uint32_t *__restrict__ mask, float inv_scale,
     double *partial)
 {
   double v[kRedVals] = { 0, 0, 0, 0, 0, 0 };
   const long long n = (long long)g.ny * g.nz;
-  const int x = g.nx - 1;
   for (long long i = (long long)blockIdx.x * kRedThreads + threadIdx.x; i < n;
        i += (long long)gridDim.x * kRedThreads) {
     const int z = (int)(i % g.nz);
     const int y = (int)(i / g.nz);
-    const long long cell = cell_index(g, x, y, z);
+    const uint32_t cell = cell_index(g, x, y, z);
     const uint32_t m = mask[cell];
     if (m & kSolidBit)
       continue;
-    Nbhd nb = make_nbhd(g, x, y, z);
+    const Offs nb = make_offs(g, x, y, z);
     double rho, jx, jy, jz;
     bool fin;
     cell_moments<ST>(g, state, orient, m, cell, nb, inv_scale, rho, jx, jy, jz, fin);
@@ -485,8 +514,6 @@ extern "C" int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *f
     return fail(LBM_ERR_ARG, "lbm_create: unknown pattern %d", pattern);
   if (precision != LBM_F64 && precision != LBM_F32 && precision != LBM_F16)
     return fail(LBM_ERR_ARG, "lbm_create: unknown precision %d", precision);
-  if (nx > 65535)
-    return fail(LBM_ERR_ARG, "lbm_create: nx = %d exceeds 65535 (one grid.z slice per x)", nx);
   int rc = need_device();
   if (rc)
     return rc;
@@ -507,15 +534,51 @@ extern "C" int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *f
   s->xforce = 1e-5;
   s->force_on = 0;
   s->fp16_scale = 16384.0;
+  {
+    const char *ns = getenv("LBM_B200_NO_SHUFFLE");
+    s->no_shuffle = (ns && ns[0] == '1') ? 1 : 0;
+  }
   cudaGetDevice(&s->device);
 
   const size_t S = storage_size(precision);
   const int zq = (int)(32 / S); // z pitch quantum: rows start on a 32-byte sector
-  s->g.nx = nx;
-  s->g.ny = ny;
-  s->g.nz = nz;
-  s->g.pz = (nz + zq - 1) / zq * zq;
-  long long cells = (long long)nx * ny * s->g.pz;
+  // a non-periodic axis whose faces hold fluid gets a one-cell solid frame
+  int frame[3] = { 0, 0, 0 };
+  const int dims[3] = { nx, ny, nz };
+  for (int a = 0; a < 3; ++a) {
+    if (s->periodic[a])
+      continue;
+    for (int x = 0; x < nx && !frame[a]; ++x)
+      for (int y = 0; y < ny && !frame[a]; ++y)
+        for (int z = 0; z < nz; ++z) {
+          const int c[3] = { x, y, z };
+          if ((c[a] == 0 || c[a] == dims[a] - 1) && flags[((long long)z * ny + y) * nx + x]) {
+            frame[a] = 1;
+            break;
+          }
+        }
+  }
+  s->ub.ox = frame[0];
+  s->ub.oy = frame[1];
+  s->ub.oz = frame[2];
+  s->ub.nx = nx;
+  s->ub.ny = ny;
+  s->ub.nz = nz;
+  s->g.nx = nx + 2 * frame[0];
+  s->g.ny = ny + 2 * frame[1];
+  s->g.nz = nz + 2 * frame[2];
+  s->g.pz = (s->g.nz + zq - 1) / zq * zq;
+  s->g.per = s->periodic[0] | (s->periodic[1] << 1) | (s->periodic[2] << 2);
+  long long cells = (long long)s->g.nx * s->g.ny * s->g.pz;
+  if (s->g.nx > 65535) {
+    free(s);
+    return fail(LBM_ERR_ARG, "lbm_create: x extent %d exceeds 65535", s->g.nx);
+  }
+  if (cells >= (1LL << 32)) {
+    free(s);
+    return fail(LBM_ERR_ARG, "lbm_create: %lld cells (with z padding) exceed the 2^32 limit "
+        "of the 32-bit cell index", cells);
+  }
   const long long pq = 256 / (long long)S;
   s->g.plane = (cells + pq - 1) / pq * pq;
   s->state_bytes = (size_t)Q * (size_t)s->g.plane * S;
@@ -552,14 +615,14 @@ extern "C" int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *f
   if (s->buf[1])
     TRYC(cudaMemsetAsync(s->buf[1], 0, s->state_bytes, s->stream));
 
-  // fluid bytes in device cell order (padding = solid), then the masks
+  // fluid bytes in device cell order (frames and padding = wall), then the masks
   std::vector<uint8_t> fluid((size_t)cells, 0);
   long long nf = 0;
   for (int x = 0; x < nx; ++x)
     for (int y = 0; y < ny; ++y)
       for (int z = 0; z < nz; ++z) {
         uint8_t f = flags[((long long)z * ny + y) * nx + x] != 0;
-        fluid[((size_t)x * ny + y) * s->g.pz + z] = f;
+        fluid[((size_t)(x + frame[0]) * s->g.ny + (y + frame[1])) * s->g.pz + z + frame[2]] = f;
         nf += f;
       }
   s->n_fluid = nf;
@@ -569,11 +632,10 @@ extern "C" int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *f
       s->stream);
   if (e == cudaSuccess) {
     Grid gp = s->g;
-    gp.nz = s->g.pz; // cover the padding too
+    gp.nz = s->g.pz; // cover the row padding too
     dim3 grid, block;
     cell_launch_shape(gp, grid, block);
-    mask_kernel<<<grid, block, 0, s->stream>>>(s->g, s->periodic[0], s->periodic[1],
-        s->periodic[2], dfluid, s->mask);
+    mask_kernel<<<grid, block, 0, s->stream>>>(s->g, dfluid, s->mask);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess)
@@ -583,8 +645,8 @@ extern "C" int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *f
     free_all(s);
     return fail(LBM_ERR_CUDA, "lbm_create: mask build failed: %s", cudaGetErrorString(e));
   }
-  // cells beyond nx*ny*pz inside the rounded plane stay unused; mark them solid
-  // so no kernel that walks the whole plane ever treats them as fluid
+  // cells beyond the box inside the rounded plane stay unused; mark them as
+  // walls so no kernel that walks the whole plane treats them as fluid
   if (s->g.plane > cells) {
     std::vector<uint32_t> pad((size_t)(s->g.plane - cells), kSolidBit);
     TRYC(cudaMemcpy(s->mask + cells, pad.data(), pad.size() * 4, cudaMemcpyHostToDevice));
@@ -650,7 +712,8 @@ extern "C" int lbm_set_porosity(lbm_solver *s, const float *porosity, double alp
   }
   for (int x = 0; x < s->nx; ++x)
     for (int y = 0; y < s->ny; ++y)
-      CUDA_TRY(cudaMemcpyAsync(s->porosity + ((size_t)x * s->ny + y) * s->g.pz,
+      CUDA_TRY(cudaMemcpyAsync(s->porosity + ((size_t)(x + s->ub.ox) * s->g.ny + (y + s->ub.oy)) *
+                                                  s->g.pz + s->ub.oz,
           porosity + ((size_t)x * s->ny + y) * s->nz, sizeof(float) * s->nz,
           cudaMemcpyHostToDevice, s->stream));
   CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -658,10 +721,20 @@ extern "C" int lbm_set_porosity(lbm_solver *s, const float *porosity, double alp
   return LBM_OK;
 }
 
+// Launch shape covering the caller's box.
+static void user_launch_shape(const lbm_solver *s, dim3 &grid, dim3 &block)
+{
+  Grid gu = s->g;
+  gu.nx = s->ub.nx;
+  gu.ny = s->ub.ny;
+  gu.nz = s->ub.nz;
+  cell_launch_shape(gu, grid, block);
+}
+
 template <class ST> static int pack_all(lbm_solver *s, const double *f)
 {
   dim3 grid, block;
-  cell_launch_shape(s->g, grid, block);
+  user_launch_shape(s, grid, block);
   const int o = orientation(s);
   const size_t plane_host = (size_t)s->nx * s->ny * s->nz;
   using Sx = typename ST::S;
@@ -669,7 +742,8 @@ template <class ST> static int pack_all(lbm_solver *s, const double *f)
   for (int d = 0; d < Q; ++d) {
     CUDA_TRY(cudaMemcpyAsync(s->staging, f + d * plane_host, sizeof(double) * plane_host,
         cudaMemcpyHostToDevice, s->stream));
-    pack_plane_kernel<ST><<<grid, block, 0, s->stream>>>(s->g, d, o, s->staging, state, s->mask,
+    pack_plane_kernel<ST><<<grid, block, 0, s->stream>>>(s->g, s->ub, d, o, s->staging, state,
+        s->mask,
         (float)(s->precision == LBM_F16 ? s->fp16_scale : 1.0), weight(d));
     CUDA_TRY(cudaGetLastError());
   }
@@ -680,13 +754,13 @@ template <class ST> static int pack_all(lbm_solver *s, const double *f)
 template <class ST> static int unpack_all(lbm_solver *s, double *f)
 {
   dim3 grid, block;
-  cell_launch_shape(s->g, grid, block);
+  user_launch_shape(s, grid, block);
   const int o = orientation(s);
   const size_t plane_host = (size_t)s->nx * s->ny * s->nz;
   using Sx = typename ST::S;
   const Sx *state = (const Sx *)state_ptr(s);
   for (int d = 0; d < Q; ++d) {
-    unpack_plane_kernel<ST><<<grid, block, 0, s->stream>>>(s->g, d, o, s->staging, state,
+    unpack_plane_kernel<ST><<<grid, block, 0, s->stream>>>(s->g, s->ub, d, o, s->staging, state,
         s->mask, (float)(s->precision == LBM_F16 ? 1.0 / s->fp16_scale : 1.0), weight(d));
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(f + d * plane_host, s->staging, sizeof(double) * plane_host,
@@ -750,25 +824,27 @@ static int launch_one(lbm_solver *s, int *kind_out)
     a.c = make_consts<double>(s);
     e = launch_step_f64(kind, force, brink, a, grid, block, s->stream);
   } else if (s->precision == LBM_F32) {
-    StepArgs<StoreF32> a;
+    StepArgs2<StoreF32> a;
     a.g = s->g;
     a.src = (const float *)src;
     a.dst = (float *)dst;
     a.mask = s->mask;
     a.porosity = s->porosity;
     a.u_save = nullptr;
-    a.c = make_consts<float>(s);
-    e = launch_step_f32(kind, force, brink, a, grid, block, s->stream);
+    a.c = make_consts2(s);
+    a.no_shuffle = s->no_shuffle;
+    e = launch_step_x2_f32(kind, force, brink, a, s->stream);
   } else {
-    StepArgs<StoreF16> a;
+    StepArgs2<StoreF16> a;
     a.g = s->g;
     a.src = (const __half *)src;
     a.dst = (__half *)dst;
     a.mask = s->mask;
     a.porosity = s->porosity;
     a.u_save = nullptr;
-    a.c = make_consts<float>(s);
-    e = launch_step_f16(kind, force, brink, a, grid, block, s->stream);
+    a.c = make_consts2(s);
+    a.no_shuffle = s->no_shuffle;
+    e = launch_step_x2_f16(kind, force, brink, a, s->stream);
   }
   if (e != cudaSuccess)
     return fail(LBM_ERR_CUDA, "step launch failed: %s", cudaGetErrorString(e));
@@ -865,13 +941,13 @@ extern "C" int lbm_time_launches(lbm_solver *s, int steps, double *ms_sum, int *
 template <class ST> static int moments_t(lbm_solver *s, double *q[4])
 {
   dim3 grid, block;
-  cell_launch_shape(s->g, grid, block);
+  user_launch_shape(s, grid, block);
   const size_t n = (size_t)s->nx * s->ny * s->nz;
   const float inv = (float)(s->precision == LBM_F16 ? 1.0 / s->fp16_scale : 1.0);
   for (int k = 0; k < 4; ++k) {
     if (!q[k])
       continue;
-    moments_kernel<ST><<<grid, block, 0, s->stream>>>(s->g, orientation(s), k,
+    moments_kernel<ST><<<grid, block, 0, s->stream>>>(s->g, s->ub, orientation(s), k,
         (const typename ST::S *)state_ptr(s), s->mask, inv, s->staging);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(q[k], s->staging, sizeof(double) * n, cudaMemcpyDeviceToHost,
@@ -952,8 +1028,10 @@ extern "C" int lbm_compare(lbm_solver *a, lbm_solver *b, double out[6])
 {
   if (!a || !b || !out)
     return fail(LBM_ERR_ARG, "lbm_compare: NULL argument");
-  if (a->nx != b->nx || a->ny != b->ny || a->nz != b->nz || a->device != b->device)
-    return fail(LBM_ERR_ARG, "lbm_compare: solvers differ in size or device");
+  if (a->nx != b->nx || a->ny != b->ny || a->nz != b->nz || a->device != b->device ||
+      a->g.nx != b->g.nx || a->g.ny != b->g.ny || a->g.nz != b->g.nz || a->ub.ox != b->ub.ox ||
+      a->ub.oy != b->ub.oy || a->ub.oz != b->ub.oz)
+    return fail(LBM_ERR_ARG, "lbm_compare: solvers differ in geometry or device");
   CUDA_TRY(cudaSetDevice(a->device));
   CUDA_TRY(cudaStreamSynchronize(b->stream));
   if (a->precision == LBM_F64)
@@ -977,7 +1055,8 @@ extern "C" int lbm_compare(lbm_solver *a, lbm_solver *b, double out[6])
 template <class ST> static void outlet_launch(lbm_solver *s)
 {
   const float inv = (float)(s->precision == LBM_F16 ? 1.0 / s->fp16_scale : 1.0);
-  outlet_kernel<ST><<<kRedBlocks, kRedThreads, 0, s->stream>>>(s->g, orientation(s),
+  outlet_kernel<ST><<<kRedBlocks, kRedThreads, 0, s->stream>>>(s->g,
+      s->ub.ox + s->ub.nx - 1, orientation(s),
       (const typename ST::S *)state_ptr(s), s->mask, inv, s->red);
 }
 

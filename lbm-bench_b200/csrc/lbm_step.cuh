@@ -2,33 +2,35 @@
 //
 // One thread per lattice cell, z (the unit-stride axis) across the lanes of
 // a warp, so every population plane is read and written in 32-wide
-// contiguous runs. Obstacle cells return after reading their mask word.
+// contiguous runs. Wall cells return after reading their mask word.
 //
 // The reference runs a dense sweep and then a serial bounce-back list pass
 // (src/kernel_pull_soa.c:94-204, src/kernel_push_soa.c:94-204,
 // src/kernel_aa_soa.c:42-278). Here the list pass disappears: a population
-// that would enter a wall is written straight back into a slot of its own
-// cell that no fluid neighbour uses, and the reader of that slot is
-// redirected there by the same mask bit. Per fluid cell and direction d
-// (bb(d) = neighbour x + c_d is a wall, F_d the body-force term):
+// that bounces off a wall is kept in a slot of its own cell that no
+// neighbour uses, and its reader is redirected there by the same mask bit.
+// Per fluid cell x and direction d, with bb(d) = "x + c_d is a wall" and
+// back(d) = bb(inv d) = "x - c_d is a wall":
 //
-//   pull     read  bb(inv d) ? src[inv d][x] : src[d][x - c_d]
-//            write dst[d][x] = out_d + (bb(d) ? F_inv d : F_d)
-//   push     read  src[d][x]
-//            write bb(d) ? dst[inv d][x] = out_d + F_inv d
-//                        : dst[d][x + c_d] = out_d + F_d
-//   AA even  read  A[d][x];  write A[inv d][x] = out_d + (bb(d) ? F_inv d : F_d)
-//   AA odd   read  bb(inv d) ? A[d][x] : A[inv d][x - c_d]
-//            write bb(d) ? A[inv d][x] = out_d + F_inv d
-//                        : A[d][x + c_d] = out_d + F_d
+//            read f_d(x)                         write out_d
+//   pull     back(d) ? src[inv d][x]             dst[d][x], + F_inv d if bb(d) else + F_d
+//                    : src[d][x - c_d]
+//   push     src[d][x]                           dst[d][x + c_d] + F_d; if bb(d) also
+//                                                dst[inv d][x] = out_d + F_inv d
+//   AA even  A[d][x]                             A[inv d][x], + F_inv d if bb(d) else + F_d
+//   AA odd   back(d) ? A[d][x]                   A[d][x + c_d] + F_d; if bb(d) also
+//                    : A[inv d][x - c_d]         A[inv d][x] = out_d + F_inv d
 //
-// Every value stored is fl(out_d + F), the same single rounding the
-// reference performs when kernelAddBodyForce (src/lbm.c:902-922) adds the
-// force to the populations a fluid cell receives, so the FP64 kernels are
-// bit-identical to the reference's. In the AA odd step each cell's read
-// set equals its write set ({(d, x + c_d) : fluid} plus {(d, x) : bounced})
-// and the sets of different cells are disjoint, so the in-place update is
-// race-free.
+// In push and AA odd the first store of a bounced population lands in the
+// wall cell's slot, which nothing reads; this keeps that store free of a
+// per-lane address choice. Every stored value is fl(out_d + F), the single
+// rounding the reference performs when kernelAddBodyForce
+// (src/lbm.c:902-922) adds the force to the populations a fluid cell
+// receives, so the FP64 kernels are bit-identical to the reference's.
+// Race freedom of the in-place AA odd step: a cell reads
+// {(e, x + c_e) : x + c_e fluid} and {(d, x) : back(d)}, and writes the same
+// sets plus wall slots; the sets of different cells are disjoint and wall
+// cells never run.
 #pragma once
 
 #include "lbm_device.cuh"
@@ -49,42 +51,79 @@ template <class ST> struct StepArgs {
   Consts<V> c;
 };
 
+// Minimum resident blocks per SM requested from the compiler (caps the
+// registers per thread: 65536 / (128 * n)).
+#ifndef LBM_MINB_F64
+#define LBM_MINB_F64 6
+#endif
+#ifndef LBM_MINB_LP
+#define LBM_MINB_LP 4
+#endif
+template <class ST, int KIND> struct StepOccupancy {
+  static constexpr int value = sizeof(typename ST::S) == 8 ? LBM_MINB_F64 : LBM_MINB_LP;
+};
+
+// Read-only loads of the two-lattice patterns may take the non-coherent
+// path; the in-place AA lattice is read and written by the same kernel.
+template <bool NC, typename S> __device__ __forceinline__ S ldg(const S *p)
+{
+  if constexpr (NC)
+    return __ldg(p);
+  else
+    return *p;
+}
+
 template <class ST, int KIND, bool FORCE, bool BRINK>
-__global__ void __launch_bounds__(kStepThreads) step_kernel(StepArgs<ST> a)
+__global__ void __launch_bounds__(kStepThreads, (StepOccupancy<ST, KIND>::value))
+    step_kernel(StepArgs<ST> a)
 {
   using S = typename ST::S;
   using V = typename ST::V;
+  constexpr bool kNC = (KIND == kPullStep || KIND == kPushStep);
   const Grid &g = a.g;
   const int z = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int x = blockIdx.z;
   if (z >= g.nz || y >= g.ny)
     return;
-  const long long cell = cell_index(g, x, y, z);
+  const uint32_t cell = cell_index(g, x, y, z);
   const uint32_t mask = a.mask[cell];
   if (mask & kSolidBit)
     return;
-
-  Nbhd nb;
-  if (KIND != kAAEvenStep)
-    nb = make_nbhd(g, x, y, z);
-
+  const Offs of = make_offs(g, x, y, z);
   const S *src = a.src;
   S *dst = a.dst;
   const long long P = g.plane;
 
   V f[Q];
+  // warp-uniform: warps none of whose cells has a wall link take branch-free
+  // addressing (the decision is the same for every lane)
+  const bool links = __any_sync(__activemask(), (mask & 0x7FFFFu) != 0u);
+  if (!links) {
 #pragma unroll
-  for (int d = 0; d < Q; ++d) {
-    const bool back = (mask >> inv(d)) & 1u; // x - c_d is a wall
-    const S *p;
-    if (KIND == kPullStep)
-      p = back ? src + inv(d) * P + cell : src + d * P + behind(nb, d);
-    else if (KIND == kPushStep || KIND == kAAEvenStep)
-      p = src + d * P + cell;
-    else
-      p = back ? src + d * P + cell : src + inv(d) * P + behind(nb, d);
-    f[d] = ST::load(p, d, a.c.inv_scale);
+    for (int d = 0; d < Q; ++d) {
+      const S *p;
+      if (KIND == kPullStep)
+        p = src + d * P + (uint32_t)(cell + of.at(inv(d)));
+      else if (KIND == kPushStep || KIND == kAAEvenStep)
+        p = src + d * P + cell;
+      else
+        p = src + inv(d) * P + (uint32_t)(cell + of.at(inv(d)));
+      f[d] = ST::decode(ldg<kNC>(p), a.c.inv_scale);
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < Q; ++d) {
+      const bool back = (mask >> inv(d)) & 1u;
+      const S *p;
+      if (KIND == kPullStep)
+        p = back ? src + inv(d) * P + cell : src + d * P + (uint32_t)(cell + of.at(inv(d)));
+      else if (KIND == kPushStep || KIND == kAAEvenStep)
+        p = src + d * P + cell;
+      else
+        p = back ? src + d * P + cell : src + inv(d) * P + (uint32_t)(cell + of.at(inv(d)));
+      f[d] = ST::decode(ldg<kNC>(p), a.c.inv_scale);
+    }
   }
 
   V kappa = V(0);
@@ -101,18 +140,26 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(StepArgs<ST> a)
 
 #pragma unroll
   for (int d = 0; d < Q; ++d) {
-    const bool bb = (mask >> d) & 1u; // x + c_d is a wall
-    V v = o[d];
-    if (FORCE)
-      v = v + (bb ? a.c.force[inv(d)] : a.c.force[d]);
-    S *p;
-    if (KIND == kPullStep)
-      p = dst + d * P + cell;
-    else if (KIND == kAAEvenStep)
-      p = dst + inv(d) * P + cell;
-    else
-      p = bb ? dst + inv(d) * P + cell : dst + d * P + nb.at(d);
-    ST::store(p, v, a.c.scale);
+    const bool bb = (mask >> d) & 1u;
+    if (KIND == kPullStep || KIND == kAAEvenStep) {
+      const V v = FORCE ? o[d] + (bb ? a.c.force[inv(d)] : a.c.force[d]) : o[d];
+      S *p = (KIND == kPullStep) ? dst + d * P + cell : dst + inv(d) * P + cell;
+      *p = ST::encode(v, a.c.scale);
+    } else {
+#ifndef LBM_STORE_MIRROR
+      // one store per population: a bounced one goes straight to (inv d, x)
+      const V v = FORCE ? o[d] + (bb ? a.c.force[inv(d)] : a.c.force[d]) : o[d];
+      S *p = bb ? dst + inv(d) * P + cell : dst + d * P + (uint32_t)(cell + of.at(d));
+      *p = ST::encode(v, a.c.scale);
+#else
+      const V v = FORCE ? o[d] + a.c.force[d] : o[d];
+      dst[d * P + (uint32_t)(cell + of.at(d))] = ST::encode(v, a.c.scale);
+      if (d != dC && links && bb) {
+        const V w = FORCE ? o[d] + a.c.force[inv(d)] : o[d];
+        dst[inv(d) * P + cell] = ST::encode(w, a.c.scale);
+      }
+#endif
+    }
   }
 }
 

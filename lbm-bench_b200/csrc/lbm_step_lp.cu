@@ -1,19 +1,30 @@
 // Reduced-precision step kernels: FP32 arithmetic on shifted populations
-// g_d = f_d - w_d, stored as FP32 or as FP16 (scaled by a power of two).
-// Multiply-add contraction is allowed here.
+// g_d = f_d - w_d, stored as FP32 or as FP16 (scaled by a power of two), two
+// cells per thread (lbm_step_x2.cuh). Multiply-add contraction is allowed.
 #include "lbm_internal.h"
+#include "lbm_step_x2.cuh"
+#include "lbm_step_x2s.cuh"
 
 namespace lbm {
 
+// The shuffle-aligned kernel serves the shifted patterns when nz is a
+// multiple of 64; AA even (all accesses local) and other extents use the
+// generic two-cell kernel.
 template <class ST, int KIND, bool FORCE, bool BRINK>
-static cudaError_t go(const StepArgs<ST> &a, dim3 grid, dim3 block, cudaStream_t st)
+static cudaError_t go(const StepArgs2<ST> &a, dim3 grid, dim3 block, cudaStream_t st)
 {
-  step_kernel<ST, KIND, FORCE, BRINK><<<grid, block, 0, st>>>(a);
+  if (KIND != kAAEvenStep && a.g.nz % 64 == 0 && !a.no_shuffle) {
+    dim3 sg, sb;
+    shuffle_launch_shape(a.g, sg, sb);
+    step_kernel_x2s<ST, KIND, FORCE, BRINK><<<sg, sb, 0, st>>>(a);
+  } else {
+    step_kernel_x2<ST, KIND, FORCE, BRINK><<<grid, block, 0, st>>>(a);
+  }
   return cudaGetLastError();
 }
 
 template <class ST, int KIND>
-static cudaError_t pick(bool force, bool brink, const StepArgs<ST> &a, dim3 grid, dim3 block,
+static cudaError_t pick(bool force, bool brink, const StepArgs2<ST> &a, dim3 grid, dim3 block,
     cudaStream_t st)
 {
   if (brink)
@@ -23,9 +34,11 @@ static cudaError_t pick(bool force, bool brink, const StepArgs<ST> &a, dim3 grid
 }
 
 template <class ST>
-static cudaError_t launch(int kind, bool force, bool brink, const StepArgs<ST> &a, dim3 grid,
-    dim3 block, cudaStream_t st)
+static cudaError_t launch(int kind, bool force, bool brink, const StepArgs2<ST> &a,
+    cudaStream_t st)
 {
+  dim3 grid, block;
+  pair_launch_shape(a.g, grid, block);
   switch (kind) {
   case kPullStep: return pick<ST, kPullStep>(force, brink, a, grid, block, st);
   case kPushStep: return pick<ST, kPushStep>(force, brink, a, grid, block, st);
@@ -35,16 +48,16 @@ static cudaError_t launch(int kind, bool force, bool brink, const StepArgs<ST> &
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_step_f32(int kind, bool force, bool brink, const StepArgs<StoreF32> &a,
-    dim3 grid, dim3 block, cudaStream_t st)
+cudaError_t launch_step_x2_f32(int kind, bool force, bool brink, const StepArgs2<StoreF32> &a,
+    cudaStream_t st)
 {
-  return launch(kind, force, brink, a, grid, block, st);
+  return launch(kind, force, brink, a, st);
 }
 
-cudaError_t launch_step_f16(int kind, bool force, bool brink, const StepArgs<StoreF16> &a,
-    dim3 grid, dim3 block, cudaStream_t st)
+cudaError_t launch_step_x2_f16(int kind, bool force, bool brink, const StepArgs2<StoreF16> &a,
+    cudaStream_t st)
 {
-  return launch(kind, force, brink, a, grid, block, st);
+  return launch(kind, force, brink, a, st);
 }
 
 } // namespace lbm

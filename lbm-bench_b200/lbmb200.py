@@ -17,7 +17,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "liblbmb200.so")
+LIB_PATH = os.environ.get("LBMB200_LIB") or os.path.join(HERE, "liblbmb200.so")
 
 PUSH, PULL, AA = 0, 1, 2
 F64, F32, F16 = 0, 1, 2

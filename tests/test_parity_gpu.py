@@ -84,6 +84,25 @@ def test_fp64_bit_identical_to_oracle_random_geometries(oracle, seed):
         assert np.all(out[:, ~m] == 0.0)
 
 
+@pytest.mark.parametrize("seed", range(4))
+def test_fluid_on_non_periodic_faces_bounces_off_the_box(oracle, seed):
+    """Flags with fluid on non-periodic faces (which the reference's own
+    geometries never produce): the outside acts as a wall, as in the oracle."""
+    rng = np.random.default_rng(50 + seed)
+    dims = tuple(int(v) for v in rng.integers(4, 15, size=3))
+    per = tuple(int(v) for v in rng.integers(0, 2, size=3))
+    nx, ny, nz = dims
+    flags = (rng.uniform(size=(nz, ny, nx)) > 0.2).astype(np.int32)
+    f0 = O.perturbed_state(flags, seed, amp=3e-3)
+    ref = oracle.run(flags, per, f0, 6, 1.15, 3 / 16, 2e-6, True)
+    m = O.fluid_mask(flags)
+    for pattern in PATTERNS:
+        out = gpu_run(flags, per, f0, 6, 1.15, 3 / 16, 2e-6, True, pattern)
+        assert np.array_equal(out[:, m], ref[:, m]), pattern
+        lp = gpu_run(flags, per, f0, 6, 1.15, 3 / 16, 2e-6, True, pattern, L.F32)
+        assert np.abs(lp[:, m] - ref[:, m]).max() < 1e-6, pattern
+
+
 def test_unaligned_z_extent_and_single_cell_rows(oracle):
     # nz = 3 (well below one sector of pitch) and nx = 1 periodic
     for dims, per in (((9, 7, 3), (1, 0, 1)), ((1, 6, 33), (1, 0, 0)), ((5, 1, 40), (0, 1, 0))):

@@ -65,3 +65,60 @@ def test_fp32_bytes_and_steps_per_launch():
             s.run(5)
             s.synchronize()
             assert s.launch_count == 5 and s.steps_done == 5
+
+
+def _random_walls(rng, dims, per, solid=0.25):
+    nx, ny, nz = dims
+    flags = (rng.uniform(size=(nz, ny, nx)) > solid).astype(np.int32)
+    if not per[0]:
+        flags[:, :, [0, -1]] = 0
+    if not per[1]:
+        flags[:, [0, -1], :] = 0
+    if not per[2]:
+        flags[[0, -1], :, :] = 0
+    return flags
+
+
+@pytest.mark.parametrize("precision", [L.F32, L.F16])
+@pytest.mark.parametrize("per", [(1, 0, 0), (1, 1, 1), (0, 1, 1)])
+def test_shuffle_aligned_kernels_equal_generic_pair_kernels(precision, per):
+    """For nz a multiple of 64 the shifted patterns run the shuffle-aligned
+    two-cell kernels; they move data differently but do the same arithmetic
+    as the generic two-cell kernels, so the states must agree bit for bit
+    (periodic and walled z, odd and even step counts)."""
+    import os
+    rng = np.random.default_rng(7)
+    dims = (9, 11, 128)
+    flags = _random_walls(rng, dims, per)
+    f0 = L.perturbed_equilibrium(flags, seed=4, amplitude=2e-3)
+    for pattern in ("aa", "pull", "push"):
+        outs = []
+        for no_shuffle in ("0", "1"):
+            os.environ["LBM_B200_NO_SHUFFLE"] = no_shuffle
+            try:
+                with L.Solver(flags, per, pattern, precision) as s:
+                    s.set_params(1.3, 3 / 16, 1e-5, True)
+                    s.set_state(f0)
+                    s.run(5)
+                    outs.append(s.get_state())
+            finally:
+                os.environ.pop("LBM_B200_NO_SHUFFLE", None)
+        assert np.array_equal(outs[0], outs[1]), pattern
+
+
+@pytest.mark.parametrize("per", [(1, 0, 0), (1, 1, 1)])
+def test_shuffle_aligned_kernels_track_the_oracle(oracle, per):
+    import oracle as O
+    rng = np.random.default_rng(11)
+    dims = (8, 10, 64)
+    flags = _random_walls(rng, dims, per)
+    f0 = O.perturbed_state(flags, 3, amp=2e-3)
+    ref = oracle.run(flags, per, f0, 7, 1.2, 1 / 12, 1e-5, True)
+    m = O.fluid_mask(flags)
+    for pattern in ("aa", "pull", "push"):
+        with L.Solver(flags, per, pattern, L.F32) as s:
+            s.set_params(1.2, 1 / 12, 1e-5, True)
+            s.set_state(f0)
+            s.run(7)
+            out = s.get_state()
+        assert np.abs(out[:, m] - ref[:, m]).max() < 1e-6, pattern
