@@ -47,7 +47,16 @@ __global__ void __launch_bounds__(kStepThreads, LBM_MINB_X2) step_kernel_x2s(Ste
   const bool fluid0 = !(m0 & kSolidBit), fluid1 = !(m1 & kSolidBit);
   if (!__any_sync(kFull, fluid0 || fluid1)) // uniform
     return;
-  const bool links = __any_sync(kFull, ((m0 | m1) & 0x7FFFFu) != 0u);
+  // directions in which any cell of the warp has a wall link (uniform)
+  const uint32_t wlinks = __reduce_or_sync(kFull, (m0 | m1) & 0x7FFFFu);
+  const bool links = wlinks != 0u;
+  // which halves of the aligned target pairs a lane owns in a z-shifted
+  // scatter (the same for every direction of one shift sign): for +1 the
+  // pair (z, z+1) takes cells (z-1, z), for -1 cells (z+1, z+2); a wall cell
+  // writes nothing, and the half fed from the next segment is written there
+  const unsigned f1bits = __ballot_sync(kFull, fluid1), f0bits = __ballot_sync(kFull, fluid0);
+  const bool up_x = lane > 0 && ((f1bits >> (lane - 1)) & 1u), up_y = fluid0;
+  const bool dn_x = fluid1, dn_y = lane < 31 && ((f0bits >> (lane + 1)) & 1u);
 
   // x/y parts of the neighbour offsets (uniform across the warp); the z
   // shift is handled by shuffles and the two edge lanes
@@ -160,41 +169,37 @@ __global__ void __launch_bounds__(kStepThreads, LBM_MINB_X2) step_kernel_x2s(Ste
       *reinterpret_cast<P *>(dst + d * PL + cell) = PT::enc(v);
       continue;
     }
-    // push / AA odd: every population to (d, x + c_d)
+    // push / AA odd: every population to (d, x + c_d); the aligned pair
+    // (z, z+1) of the target row is written whole where this lane owns both
+    // halves, otherwise half by half (independent predicated stores)
     const float2 v = FORCE ? add2(out[d], f2(a.c.force[d])) : out[d];
     S *base = dst + d * PL + (uint32_t)(cell + row(d));
     float2 t;
-    bool tx, ty; // which halves of the aligned target pair this lane writes
+    bool tx, ty;
     if (cz(d) == 0) {
       t = v;
       tx = fluid0;
       ty = fluid1;
-    } else if (cz(d) > 0) { // targets z + 1, z + 2: pair (z, z+1) <- cells (z-1, z)
-      const float up = __shfl_up_sync(kFull, v.y, 1);
-      const bool upf = __shfl_up_sync(kFull, (int)fluid1, 1) != 0;
-      t = make_float2(up, v.x);
-      tx = lane > 0 && upf;
-      ty = fluid0;
-      if (lane == 31 && fluid1) // leftover: cell z+1 -> z+2 (next segment)
+    } else if (cz(d) > 0) { // targets z + 1, z + 2
+      t = make_float2(__shfl_up_sync(kFull, v.y, 1), v.x);
+      tx = up_x;
+      ty = up_y;
+      if (lane == 31 && fluid1) // cell z+1 -> z+2, first element of the next segment
         base[hi] = PT::enc1(v.y);
-    } else { // targets z - 1, z: pair (z, z+1) <- cells (z+1, z+2)
-      const float dn = __shfl_down_sync(kFull, v.x, 1);
-      const bool dnf = __shfl_down_sync(kFull, (int)fluid0, 1) != 0;
-      t = make_float2(v.y, dn);
-      tx = fluid1;
-      ty = lane < 31 && dnf;
-      if (lane == 0 && fluid0) // leftover: cell z -> z-1 (previous segment)
+    } else { // targets z - 1, z
+      t = make_float2(v.y, __shfl_down_sync(kFull, v.x, 1));
+      tx = dn_x;
+      ty = dn_y;
+      if (lane == 0 && fluid0) // cell z -> z-1, last element of the previous segment
         base[lo] = PT::enc1(v.x);
     }
-    if (tx && ty) {
+    if (tx && ty)
       *reinterpret_cast<P *>(base) = PT::enc(t);
-    } else {
-      if (tx)
-        base[0] = PT::enc1(t.x);
-      if (ty)
-        base[1] = PT::enc1(t.y);
-    }
-    if (d != dC && links) {
+    if (tx && !ty)
+      base[0] = PT::enc1(t.x);
+    if (ty && !tx)
+      base[1] = PT::enc1(t.y);
+    if (d != dC && ((wlinks >> d) & 1u)) {
       // bounce-back: the bounced value into (inv d, x)
       const float2 w = FORCE ? add2(out[d], f2(a.c.force[inv(d)])) : out[d];
       S *ob = dst + inv(d) * PL + cell;
