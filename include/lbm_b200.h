@@ -89,6 +89,24 @@ int lbm_set_porosity(lbm_solver *s, const float *porosity, double alpha);
 int lbm_set_state(lbm_solver *s, const double *f);
 int lbm_get_state(lbm_solver *s, double *f);
 
+/* Orientation of a state held in LBM-Bench's own padded SoA array
+ * (indexSoA with a one-cell ghost layer, (nx+2)*(ny+2)*(nz+2) values per
+ * direction, src/lbm.h:113-116): where kd->GetNode finds f_d(x)
+ * (src/lbm.c:193-294). NATURAL: push kernels, AA before its first and
+ * after every odd iteration; PULL: pull kernels; AA_EVEN: AA after an even
+ * iteration. */
+#define LBM_REF_NATURAL 0
+#define LBM_REF_PULL 1
+#define LBM_REF_AA_EVEN 2
+
+/* Uploads / downloads the state from / to an array in the reference's
+ * padded layout and the given orientation; elem_size 8 (PdfType double) or
+ * 4 (float, the reference's PRECISION_SP build). Only the slots GetNode
+ * reads for fluid cells are used; on download every other slot is set to 0.
+ * Replaces the host-side SetNode/GetNode loops around a kd->Kernel call. */
+int lbm_set_state_padded(lbm_solver *s, const void *pdfs, int elem_size, int ref_orientation);
+int lbm_get_state_padded(lbm_solver *s, void *pdfs, int elem_size, int ref_orientation);
+
 /* Enqueues `steps` time steps on the solver's stream (asynchronous).
  * Replaces the time loop of kd->Kernel (src/kernel_pull_soa.c:44-214,
  * src/kernel_push_soa.c:44-214, src/kernel_aa_soa.c:36-286); an AA solver

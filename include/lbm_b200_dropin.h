@@ -1,0 +1,133 @@
+/* liblbmb200 drop-in kernels for LBM-Bench's kernel registry.
+ *
+ * LBM-Bench selects a kernel by name from GKernels[] = {Name, Init, Deinit}
+ * (src/lbm.c:33-41, type at src/lbm.h:99-103); Init fills a KernelDataType
+ * whose Kernel member runs the time loop (src/lbm.h:96), and the driver
+ * reads and writes populations through kd->GetNode / kd->SetNode
+ * (src/lbm.c:193-294). The functions below have exactly those signatures, so
+ * a maintainer adds rows such as
+ *     { "cuda-aa-soa", kernelInitCudaAaSoA, kernelDeinitCuda },
+ * to GKernels[] and links liblbmb200.
+ *
+ * The kernel data the Init functions return keeps the reference's host
+ * arrays (Pdfs[0..1] in the padded indexSoA layout, page-locked) and
+ * accessors; Kernel copies PdfsActive to the GPU, runs cd->MaxIterations
+ * steps there (AA: rounded up to an even count, as src/kernel_aa_soa.c:36
+ * does), times only the step loop into kd->Duration, and copies the result
+ * back into the array the reference would end in. BounceBackPdfsSrc/Dst are
+ * NULL (the GPU uses per-cell link masks); nBounceBackPdfs holds the count
+ * the reference would list. LoopBalance is 2*19*sizeof(PdfType) for every
+ * pattern (the reference's AA value, src/lbm.c:657, counts half the
+ * traffic).
+ *
+ * Errors follow the reference's style: a message on stdout and
+ * exit(EXIT_FAILURE) (src/allocate.c:14-27).
+ */
+#ifndef LBM_B200_DROPIN_H
+#define LBM_B200_DROPIN_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The reference's types (src/lbm.h:10-106), declared here only when its
+ * lbm.h has not been included; field order and types are the ABI. */
+#ifndef __LBM_H_
+#ifdef PRECISION_SP
+typedef float PdfType;
+#else
+typedef double PdfType;
+#endif
+typedef int LatticeType;
+
+typedef struct LatticeDesc {
+  int Dims[3];
+  LatticeType *Lattice;
+  int nCells;
+  int nFluid;
+  int nObst;
+  int nInlet;
+  int nOutlet;
+  int PeriodicX;
+  int PeriodicY;
+  int PeriodicZ;
+  const char *Name;
+} LatticeDescType;
+
+typedef struct CaseData {
+  PdfType Omega;
+  PdfType RhoIn;
+  PdfType RhoOut;
+  PdfType XForce;
+  int MaxIterations;
+  int StatisticsModulus;
+} CaseDataType;
+
+typedef struct KernelData {
+  PdfType *Pdfs[2];
+  PdfType *PdfsActive;
+  int Dims[3];
+  int GlobalDims[3];
+  int Offsets[3];
+  int *BounceBackPdfsSrc;
+  int *BounceBackPdfsDst;
+  int nBounceBackPdfs;
+  int Blk[3];
+  int Iteration;
+  double LoopBalance;
+  double Duration;
+  void (*GetNode)(struct KernelData *kd, int x, int y, int z, PdfType *pdfs);
+  void (*SetNode)(struct KernelData *kd, int x, int y, int z, PdfType *pdfs);
+  void (*BoundaryConditionsGetPdf)(
+      struct KernelData *kd, int x, int y, int z, int dir, PdfType *pdf);
+  void (*BoundaryConditionsSetPdf)(
+      struct KernelData *kd, int x, int y, int z, int dir, PdfType pdf);
+  void (*Kernel)(LatticeDescType *ld, struct KernelData *kd, CaseDataType *cd);
+} KernelDataType;
+
+typedef struct KernelFunctions {
+  const char *Name;
+  void (*Init)(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
+  void (*Deinit)(LatticeDescType *ld, KernelDataType **kd);
+} KernelFunctionsType;
+#endif
+
+/* Init functions (replace kernelInitPullSoA / kernelInitPushSoA /
+ * kernelInitAaSoA, src/lbm.c:601-658). The plain names compute in the
+ * library's PdfType precision (FP64 in a double build, FP32 with shifted
+ * storage in a PRECISION_SP build); the _Fp32 / _Fp16 names select FP32
+ * arithmetic with shifted FP32 / FP16 storage whatever PdfType is. */
+void kernelInitCudaPullSoA(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
+void kernelInitCudaPushSoA(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
+void kernelInitCudaAaSoA(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
+void kernelInitCudaPullSoAFp32(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
+void kernelInitCudaPushSoAFp32(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
+void kernelInitCudaAaSoAFp32(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
+void kernelInitCudaPullSoAFp16(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
+void kernelInitCudaPushSoAFp16(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
+void kernelInitCudaAaSoAFp16(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
+
+/* Deinit for all of them (replaces kernelDeinit, src/lbm.c:660-670). */
+void kernelDeinitCuda(LatticeDescType *ld, KernelDataType **kd);
+
+/* All rows above as a ready-made table, for drivers that list or look up
+ * kernels the way src/main.c:93-99 and src/cli.c:79-83 do. */
+extern const KernelFunctionsType LbmB200Kernels[];
+extern const int LBM_B200_N_KERNELS;
+
+/* TRT magic parameter Lambda (the reference hard-codes 1/12,
+ * src/kernel_pull_soa.c:20); default 1/12. */
+void lbmB200SetMagicParameter(double lambda);
+
+/* Whether Kernel adds the Luo body force cd->XForce after every step, as the
+ * reference's -DVERIFICATION build does (src/kernel_pull_soa.c:206-209):
+ * 1 on, 0 off, -1 (default) from the environment variable
+ * LBM_B200_BODY_FORCE ("1" = on, anything else or unset = off, the
+ * reference's benchmark build). */
+void lbmB200SetBodyForce(int on);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

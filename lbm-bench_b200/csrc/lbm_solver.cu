@@ -60,6 +60,8 @@ struct lbm_solver {
   float *porosity;
   double alpha;
   double *staging; // one dense plane, nx*ny*nz doubles
+  void *pstaging;  // one plane of the reference's padded layout (allocated on first use)
+  size_t pstaging_bytes;
   double *red;     // reduction partials
   long long n_fluid;
   double omega, lambda, xforce;
@@ -475,6 +477,7 @@ static void free_all(lbm_solver *s)
   cudaFree(s->mask);
   cudaFree(s->porosity);
   cudaFree(s->staging);
+  cudaFree(s->pstaging);
   cudaFree(s->red);
   if (s->ev[0])
     cudaEventDestroy(s->ev[0]);
@@ -792,6 +795,156 @@ extern "C" int lbm_get_state(lbm_solver *s, double *f)
   case LBM_F32: return unpack_all<StoreF32>(s, f);
   default: return unpack_all<StoreF16>(s, f);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Transfers in the reference's own padded layout (for the drop-in kernels)
+// ---------------------------------------------------------------------------
+
+// Slot of f_d(x) in the reference's padded SoA array, relative to one
+// direction plane (indexSoA, src/lbm.h:113-116, ghost offset 1): push and
+// AA odd/initial states keep f_d(x) at (x, d), pull at (x - c_d, d), AA
+// after an even iteration at (x - c_d, inv d) (src/lbm.c:193-294). For a
+// padded plane p the kernel handles direction d = p, or inv p in the AA
+// even orientation.
+__device__ __forceinline__ long long ref_index(int rx, int ry, int rz, int ref_orient, int d,
+    int x, int y, int z)
+{
+  int a = x + 1, b = y + 1, c = z + 1;
+  if (ref_orient != LBM_REF_NATURAL) {
+    a -= cx(d);
+    b -= cy(d);
+    c -= cz(d);
+  }
+  return ((long long)a * ry + b) * rz + c;
+}
+
+template <class ST, typename H>
+__global__ void pack_ref_kernel(Grid g, UserBox u, int p, int ref_orient, int orient,
+    const H *__restrict__ plane, typename ST::S *state, const uint32_t *__restrict__ mask,
+    float scale)
+{
+  using V = typename ST::V;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= u.nz || y >= u.ny)
+    return;
+  const uint32_t cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
+  const uint32_t m = mask[cell];
+  if (m & kSolidBit)
+    return;
+  const int d = (ref_orient == LBM_REF_AA_EVEN) ? inv(p) : p;
+  const Offs nb = make_offs(g, x + u.ox, y + u.oy, z + u.oz);
+  int sp;
+  uint32_t sc;
+  state_slot(orient, d, m, cell, nb, sp, sc);
+  double v = (double)plane[ref_index(u.nx + 2, u.ny + 2, u.nz + 2, ref_orient, d, x, y, z)];
+  if (ST::kShifted) {
+    const int wc = wclass(d);
+    v -= wc == 0 ? 1.0 / 3.0 : wc == 1 ? 1.0 / 18.0 : 1.0 / 36.0;
+  }
+  ST::store(state + (long long)sp * g.plane + sc, (V)v, (V)scale);
+}
+
+template <class ST, typename H>
+__global__ void unpack_ref_kernel(Grid g, UserBox u, int p, int ref_orient, int orient,
+    H *__restrict__ plane, const typename ST::S *state, const uint32_t *__restrict__ mask,
+    float inv_scale)
+{
+  using V = typename ST::V;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= u.nz || y >= u.ny)
+    return;
+  const uint32_t cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
+  const uint32_t m = mask[cell];
+  if (m & kSolidBit)
+    return;
+  const int d = (ref_orient == LBM_REF_AA_EVEN) ? inv(p) : p;
+  const Offs nb = make_offs(g, x + u.ox, y + u.oy, z + u.oz);
+  int sp;
+  uint32_t sc;
+  state_slot(orient, d, m, cell, nb, sp, sc);
+  double v = (double)ST::load(state + (long long)sp * g.plane + sc, d, (V)inv_scale);
+  if (ST::kShifted) {
+    const int wc = wclass(d);
+    v += wc == 0 ? 1.0 / 3.0 : wc == 1 ? 1.0 / 18.0 : 1.0 / 36.0;
+  }
+  plane[ref_index(u.nx + 2, u.ny + 2, u.nz + 2, ref_orient, d, x, y, z)] = (H)v;
+}
+
+template <class ST, typename H>
+static int ref_transfer(lbm_solver *s, void *host, int ref_orient, bool upload)
+{
+  const size_t gpl = (size_t)(s->nx + 2) * (s->ny + 2) * (s->nz + 2);
+  const size_t bytes = gpl * sizeof(H);
+  if (s->pstaging_bytes < bytes) {
+    cudaFree(s->pstaging);
+    s->pstaging = NULL;
+    s->pstaging_bytes = 0;
+    int rc = dev_alloc(s, &s->pstaging, bytes, "the padded transfer plane");
+    if (rc)
+      return rc;
+    s->pstaging_bytes = bytes;
+  }
+  dim3 grid, block;
+  user_launch_shape(s, grid, block);
+  const int o = orientation(s);
+  const float sc = (float)(s->precision == LBM_F16 ? s->fp16_scale : 1.0);
+  using Sx = typename ST::S;
+  H *hp = (H *)host;
+  H *dp = (H *)s->pstaging;
+  for (int p = 0; p < Q; ++p) {
+    if (upload) {
+      CUDA_TRY(cudaMemcpyAsync(dp, hp + p * gpl, bytes, cudaMemcpyHostToDevice, s->stream));
+      pack_ref_kernel<ST, H><<<grid, block, 0, s->stream>>>(s->g, s->ub, p, ref_orient, o, dp,
+          (Sx *)state_ptr(s), s->mask, sc);
+      CUDA_TRY(cudaGetLastError());
+    } else {
+      // slots that hold no fluid population come back as 0
+      CUDA_TRY(cudaMemsetAsync(dp, 0, bytes, s->stream));
+      unpack_ref_kernel<ST, H><<<grid, block, 0, s->stream>>>(s->g, s->ub, p, ref_orient, o, dp,
+          (const Sx *)state_ptr(s), s->mask, 1.0f / sc);
+      CUDA_TRY(cudaGetLastError());
+      CUDA_TRY(cudaMemcpyAsync(hp + p * gpl, dp, bytes, cudaMemcpyDeviceToHost, s->stream));
+    }
+  }
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return LBM_OK;
+}
+
+static int ref_dispatch(lbm_solver *s, void *host, int elem_size, int ref_orient, bool upload)
+{
+  if (!s || !host || (elem_size != 8 && elem_size != 4) || ref_orient < LBM_REF_NATURAL ||
+      ref_orient > LBM_REF_AA_EVEN)
+    return fail(LBM_ERR_ARG, "padded transfer: bad arguments");
+  CUDA_TRY(cudaSetDevice(s->device));
+  if (elem_size == 8) {
+    if (s->precision == LBM_F64)
+      return ref_transfer<StoreF64, double>(s, host, ref_orient, upload);
+    if (s->precision == LBM_F32)
+      return ref_transfer<StoreF32, double>(s, host, ref_orient, upload);
+    return ref_transfer<StoreF16, double>(s, host, ref_orient, upload);
+  }
+  if (s->precision == LBM_F64)
+    return ref_transfer<StoreF64, float>(s, host, ref_orient, upload);
+  if (s->precision == LBM_F32)
+    return ref_transfer<StoreF32, float>(s, host, ref_orient, upload);
+  return ref_transfer<StoreF16, float>(s, host, ref_orient, upload);
+}
+
+extern "C" int lbm_set_state_padded(lbm_solver *s, const void *pdfs, int elem_size,
+    int ref_orientation)
+{
+  return ref_dispatch(s, const_cast<void *>(pdfs), elem_size, ref_orientation, true);
+}
+
+extern "C" int lbm_get_state_padded(lbm_solver *s, void *pdfs, int elem_size,
+    int ref_orientation)
+{
+  return ref_dispatch(s, pdfs, elem_size, ref_orientation, false);
 }
 
 // Launches one step and advances the bookkeeping.

@@ -288,3 +288,143 @@ def perturbed_equilibrium(flags, seed=1, amplitude=1e-4, rho=1.0):
     _check(lib().lbm_perturbed_equilibrium(nx, ny, nz, _p(flags, _ip), seed, amplitude, rho,
                                            _p(f, _dp)))
     return f
+
+
+
+# ---------------------------------------------------------------------------
+# drop-in kernels through the reference's own structs (lbm_b200_dropin.h)
+# ---------------------------------------------------------------------------
+
+class LatticeDesc(ctypes.Structure):
+    """LatticeDescType of the reference (src/lbm.h:54-66)."""
+    _fields_ = [("Dims", ctypes.c_int * 3), ("Lattice", ctypes.POINTER(ctypes.c_int)),
+                ("nCells", ctypes.c_int), ("nFluid", ctypes.c_int), ("nObst", ctypes.c_int),
+                ("nInlet", ctypes.c_int), ("nOutlet", ctypes.c_int), ("PeriodicX", ctypes.c_int),
+                ("PeriodicY", ctypes.c_int), ("PeriodicZ", ctypes.c_int),
+                ("Name", ctypes.c_char_p)]
+
+
+class CaseData(ctypes.Structure):
+    """CaseDataType of the reference's double build (src/lbm.h:68-75)."""
+    _fields_ = [("Omega", ctypes.c_double), ("RhoIn", ctypes.c_double),
+                ("RhoOut", ctypes.c_double), ("XForce", ctypes.c_double),
+                ("MaxIterations", ctypes.c_int), ("StatisticsModulus", ctypes.c_int)]
+
+
+class KernelData(ctypes.Structure):
+    pass
+
+
+_node_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(KernelData), ctypes.c_int, ctypes.c_int,
+                            ctypes.c_int, ctypes.POINTER(ctypes.c_double))
+_bcget_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(KernelData), ctypes.c_int, ctypes.c_int,
+                             ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double))
+_bcset_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(KernelData), ctypes.c_int, ctypes.c_int,
+                             ctypes.c_int, ctypes.c_int, ctypes.c_double)
+_kernel_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(LatticeDesc), ctypes.POINTER(KernelData),
+                              ctypes.POINTER(CaseData))
+KernelData._fields_ = [
+    ("Pdfs", ctypes.POINTER(ctypes.c_double) * 2), ("PdfsActive", ctypes.POINTER(ctypes.c_double)),
+    ("Dims", ctypes.c_int * 3), ("GlobalDims", ctypes.c_int * 3), ("Offsets", ctypes.c_int * 3),
+    ("BounceBackPdfsSrc", ctypes.POINTER(ctypes.c_int)),
+    ("BounceBackPdfsDst", ctypes.POINTER(ctypes.c_int)), ("nBounceBackPdfs", ctypes.c_int),
+    ("Blk", ctypes.c_int * 3), ("Iteration", ctypes.c_int), ("LoopBalance", ctypes.c_double),
+    ("Duration", ctypes.c_double), ("GetNode", _node_fn), ("SetNode", _node_fn),
+    ("BoundaryConditionsGetPdf", _bcget_fn), ("BoundaryConditionsSetPdf", _bcset_fn),
+    ("Kernel", _kernel_fn)]
+
+_init_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(LatticeDesc),
+                            ctypes.POINTER(ctypes.POINTER(KernelData)), ctypes.POINTER(CaseData))
+_deinit_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(LatticeDesc),
+                              ctypes.POINTER(ctypes.POINTER(KernelData)))
+
+
+class KernelFunctions(ctypes.Structure):
+    _fields_ = [("Name", ctypes.c_char_p), ("Init", _init_fn), ("Deinit", _deinit_fn)]
+
+
+def _registry():
+    L = lib()
+    n = ctypes.c_int.in_dll(L, "LBM_B200_N_KERNELS").value
+    return (KernelFunctions * n).in_dll(L, "LbmB200Kernels")
+
+
+def dropin_kernels():
+    """Names in the library's registry (LbmB200Kernels)."""
+    return [k.Name.decode() for k in _registry()]
+
+
+class DropIn:
+    """One kernel of the drop-in registry driven the way LBM-Bench's driver
+    drives a kernel (src/main.c:93-152): look up by name, Init, SetNode,
+    Kernel, GetNode, Deinit."""
+
+    def __init__(self, name, flags, periodic, omega=1.0, xforce=1e-5, iterations=10,
+                 force_on=None, lam=None):
+        L = lib()
+        self.kf = next((k for k in _registry() if k.Name.decode() == name), None)
+        if self.kf is None:
+            raise KeyError(name)
+        L.lbmB200SetBodyForce.argtypes = [ctypes.c_int]
+        L.lbmB200SetMagicParameter.argtypes = [ctypes.c_double]
+        L.lbmB200SetBodyForce(-1 if force_on is None else int(force_on))
+        L.lbmB200SetMagicParameter(1.0 / 12.0 if lam is None else lam)
+        self.flags = np.ascontiguousarray(flags, dtype=np.int32)
+        nz, ny, nx = self.flags.shape
+        self.shape = (nx, ny, nz)
+        self.ld = LatticeDesc()
+        self.ld.Dims[:] = [nx, ny, nz]
+        self.ld.Lattice = self.flags.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        self.ld.nCells = nx * ny * nz
+        self.ld.nFluid = int((self.flags != 0).sum())
+        self.ld.nObst = self.ld.nCells - self.ld.nFluid
+        self.ld.PeriodicX, self.ld.PeriodicY, self.ld.PeriodicZ = (int(p) for p in periodic)
+        self.ld.Name = b"python"
+        self.cd = CaseData(omega, 1.0, 1.0, xforce, iterations, 100)
+        self.kd = ctypes.POINTER(KernelData)()
+        self.kf.Init(ctypes.byref(self.ld), ctypes.byref(self.kd), ctypes.byref(self.cd))
+        self._buf = (ctypes.c_double * Q)()
+
+    @property
+    def data(self) -> KernelData:
+        return self.kd.contents
+
+    def pdfs(self, which: int) -> np.ndarray:
+        """Zero-copy view of kd->Pdfs[which], shape [19, nx+2, ny+2, nz+2]."""
+        g = tuple(self.data.GlobalDims)
+        n = Q * g[0] * g[1] * g[2]
+        return np.ctypeslib.as_array(self.data.Pdfs[which], shape=(n,)).reshape((Q,) + g)
+
+    def set_state(self, f):
+        """f[19, nx, ny, nz] for fluid cells, written through kd->SetNode."""
+        fl = np.transpose(self.flags, (2, 1, 0)) != 0
+        for x, y, z in np.argwhere(fl):
+            self._buf[:] = f[:, x, y, z]
+            self.data.SetNode(self.kd, int(x), int(y), int(z), self._buf)
+
+    def get_state(self):
+        """f[19, nx, ny, nz] read through kd->GetNode (0 on obstacles)."""
+        out = np.zeros((Q,) + self.shape)
+        fl = np.transpose(self.flags, (2, 1, 0)) != 0
+        for x, y, z in np.argwhere(fl):
+            self.data.GetNode(self.kd, int(x), int(y), int(z), self._buf)
+            out[:, x, y, z] = self._buf[:]
+        return out
+
+    def run(self, iterations=None):
+        """kd->Kernel(ld, kd, cd); returns kd->Duration (s, step loop only)."""
+        if iterations is not None:
+            self.cd.MaxIterations = int(iterations)
+        self.data.Kernel(ctypes.byref(self.ld), self.kd, ctypes.byref(self.cd))
+        return self.data.Duration
+
+    def close(self):
+        if getattr(self, "kd", None):
+            self.kf.Deinit(ctypes.byref(self.ld), ctypes.byref(self.kd))
+            self.kd = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -1,0 +1,82 @@
+"""The drop-in boundary without a GPU: the reference-ABI structs of
+include/lbm_b200_dropin.h against LBM-Bench's own src/lbm.h, the registry,
+the ctypes mirror, and the lbmbench-b200 driver's CLI."""
+import ctypes
+import os
+import subprocess
+
+import pytest
+
+import lbmb200 as L
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "lbm-bench_b200")
+CLI = os.path.join(PKG, "lbmbench-b200")
+PROBE = os.path.join(ROOT, "tests", "dropin_layout_probe.c")
+REF_SRC = "/root/reference/src"
+
+
+def _probe(tmp_path, *flags):
+    exe = tmp_path / ("probe" + "_".join(f.strip("-").replace("/", "") for f in flags))
+    cmd = ["gcc", "-std=gnu11", "-I", os.path.join(ROOT, "include"), *flags, PROBE, "-o",
+           str(exe), "-L", PKG, "-llbmb200", f"-Wl,-rpath,{PKG}"]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    return subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+
+
+def test_dropin_types_compile_and_link_standalone(tmp_path):
+    out = _probe(tmp_path)
+    assert "rows 3" in out
+    assert "sizeof PdfType 8" in out
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_SRC, "lbm.h")),
+                    reason="reference sources not mounted here")
+@pytest.mark.parametrize("sp", [False, True])
+def test_dropin_struct_layout_equals_reference_lbm_h(tmp_path, sp):
+    extra = ["-DPRECISION_SP"] if sp else []
+    ours = _probe(tmp_path, *extra)
+    theirs = _probe(tmp_path, "-DWITH_REFERENCE_HEADER", "-I", REF_SRC, *extra)
+    assert ours == theirs
+
+
+def test_ctypes_mirror_matches_the_c_layout(tmp_path):
+    out = dict(line.rsplit(" ", 1) for line in _probe(tmp_path).splitlines())
+    assert int(out["sizeof KernelDataType"]) == ctypes.sizeof(L.KernelData)
+    assert int(out["sizeof LatticeDescType"]) == ctypes.sizeof(L.LatticeDesc)
+    assert int(out["sizeof CaseDataType"]) == ctypes.sizeof(L.CaseData)
+    assert int(out["KernelDataType.Kernel"]) == L.KernelData.Kernel.offset
+    assert int(out["KernelDataType.Duration"]) == L.KernelData.Duration.offset
+
+
+def test_registry_names():
+    names = L.dropin_kernels()
+    assert names[:3] == ["cuda-pull-soa", "cuda-push-soa", "cuda-aa-soa"]
+    assert len(names) == 9 and len(set(names)) == 9
+
+
+def test_cli_lists_kernels_like_the_reference():
+    out = subprocess.run([CLI, "-l"], capture_output=True, text=True, check=True).stdout
+    # the reference's test.sh parses -l this way (src/test.sh:95)
+    lines = out.splitlines()
+    start = lines.index("Available kernels:")
+    assert [ln.split()[0] for ln in lines[start + 1:] if ln.strip()] == L.dropin_kernels()
+
+
+def test_cli_rejects_bad_input():
+    r = subprocess.run([CLI, "-d", "8x0x8"], capture_output=True, text=True)
+    assert r.returncode != 0 and "ERROR: Y dimension must be > 0." in r.stdout
+    r = subprocess.run([CLI, "-d", "8x8x8", "-k", "no-such-kernel"], capture_output=True,
+                       text=True)
+    assert r.returncode == 1 and 'ERROR: kernel "no-such-kernel" not found.' in r.stdout
+    r = subprocess.run([CLI, "-g", "sphere"], capture_output=True, text=True)
+    assert r.returncode != 0 and "unknown geometry type" in r.stdout
+    r = subprocess.run([CLI, "-h"], capture_output=True, text=True, check=True)
+    assert "-V                   Run verification" in r.stdout
+
+
+@pytest.mark.skipif(L.device_count() > 0, reason="a CUDA device is present")
+def test_cli_fails_loudly_without_gpu():
+    r = subprocess.run([CLI, "-d", "8x8x8"], capture_output=True, text=True)
+    assert r.returncode != 0
+    assert "no CPU path" in r.stdout

@@ -1,0 +1,97 @@
+"""The drop-in kernels driven through LBM-Bench's own structs and calling
+sequence (Init, SetNode, Kernel, GetNode, Deinit), on a B200: bit-identical
+to the reference's kernels on the golden fixtures, and the lbmbench-b200
+driver's -V Poiseuille run for every registered kernel."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import golden_io
+import lbmb200 as L
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "lbm-bench_b200", "lbmbench-b200")
+CASES, _ = golden_io.load()
+STEP_CASES = [c for c in CASES if "verify" not in c]
+
+
+@pytest.mark.parametrize("kernel", ["cuda-pull-soa", "cuda-push-soa", "cuda-aa-soa"])
+@pytest.mark.parametrize("case", STEP_CASES, ids=[c["name"] for c in STEP_CASES])
+def test_dropin_bit_identical_to_reference_fixtures(golden, case, kernel):
+    _, arrays = golden
+    flags = golden_io.build_flags(case, arrays)
+    f0 = golden_io.initial_state(case, flags)
+    with L.DropIn(kernel, flags, case["periodic"], omega=case["omega"], xforce=case["xforce"],
+                  iterations=case["steps"], force_on=bool(case["force_on"]),
+                  lam=case["lambda"]) as k:
+        k.set_state(f0)
+        k.run()
+        out = k.get_state()
+        data = k.data
+        assert data.Duration > 0.0
+        if kernel == "cuda-aa-soa":
+            assert data.Iteration == case["steps"] - 1
+    assert golden_io.state_digest(out, flags) == case["sha256"]
+
+
+def test_dropin_ends_in_the_buffer_the_reference_ends_in():
+    flags, per, _ = L.geometry("channel", (10, 9, 8))
+    f0 = L.perturbed_equilibrium(flags, seed=3)
+    with L.DropIn("cuda-pull-soa", flags, per, omega=1.2, iterations=3, force_on=True) as k:
+        k.set_state(f0)
+        k.run()
+        # three pointer swaps: the state is in Pdfs[1] (src/kernel_pull_soa.c:211-217)
+        addr = lambda p: ctypes.cast(p, ctypes.c_void_p).value  # noqa: E731
+        assert addr(k.data.PdfsActive) == addr(k.data.Pdfs[1])
+        # the oracle agrees with what GetNode reads
+        ref = O.Oracle().run(flags, per, f0, 3, 1.2, 1 / 12, 1e-5, True)
+        m = O.fluid_mask(flags)
+        assert np.array_equal(k.get_state()[:, m], ref[:, m])
+
+
+def test_dropin_aa_odd_iteration_count_runs_pairs():
+    flags, per, _ = L.geometry("channel", (8, 7, 9))
+    f0 = L.perturbed_equilibrium(flags, seed=5)
+    with L.DropIn("cuda-aa-soa", flags, per, omega=1.1, iterations=5, force_on=True) as k:
+        k.set_state(f0)
+        k.run()
+        assert k.data.Iteration == 5  # six steps, as src/kernel_aa_soa.c:36 runs them
+        ref = O.Oracle().run(flags, per, f0, 6, 1.1, 1 / 12, 1e-5, True)
+        m = O.fluid_mask(flags)
+        assert np.array_equal(k.get_state()[:, m], ref[:, m])
+
+
+def test_dropin_reduced_precision_tracks_fp64():
+    flags, per, _ = L.geometry("blocks-4", (24, 20, 18))
+    f0 = L.perturbed_equilibrium(flags, seed=9, amplitude=1e-3)
+    m = O.fluid_mask(flags)
+    ref = O.Oracle().run(flags, per, f0, 10, 1.3, 1 / 12, 1e-5, True)
+    for name, tol in (("cuda-aa-soa-fp32", 1e-6), ("cuda-pull-soa-fp16", 2e-4)):
+        with L.DropIn(name, flags, per, omega=1.3, iterations=10, force_on=True) as k:
+            k.set_state(f0)
+            k.run()
+            out = k.get_state()
+        assert np.abs(out[:, m] - ref[:, m]).max() < tol, name
+
+
+@pytest.mark.parametrize("kernel", L.dropin_kernels() if os.path.exists(L.LIB_PATH) else [])
+def test_cli_verification_run_succeeds(kernel):
+    """The reference's test.sh runs `lbmbench -V -k K` for every kernel `-l`
+    lists and requires exit status 0 (src/test.sh:61-74, 101-103)."""
+    r = subprocess.run([CLI, "-V", "-k", kernel], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "# VERIFICATION SUCCEEDED." in r.stdout
+    err = float(re.search(r"deviation from analytical solution: (\S+)", r.stdout).group(1))
+    if kernel in ("cuda-pull-soa", "cuda-push-soa", "cuda-aa-soa"):
+        # the reference's own -V run on this case gives 4.5614e-02 (golden fixture)
+        ref = next(c for c in CASES if c["name"] == "poiseuille_V")["verify"]["aa-soa"]
+        assert err == pytest.approx(ref["error_norm"], rel=1e-6)
+    else:
+        assert err < 0.06
