@@ -176,6 +176,21 @@ int lbm_compare(lbm_solver *a, lbm_solver *b, double out[6]);
  * momentum. No counterpart in the reference. */
 int lbm_objective(lbm_solver *s, double *j);
 
+/* Gradient of J (lbm_objective) after `steps` Brinkman steps from the
+ * current state, with respect to the porosity field: the discrete adjoint
+ * of the step, reverse in time. AA solvers with FP64 or FP32 storage and a
+ * porosity field set (lbm_set_porosity). The forward sweep keeps a
+ * checkpoint every `checkpoint_every` steps (0: the interval that minimises
+ * checkpoint plus segment memory, about sqrt(steps * state / momentum)); the
+ * reverse sweep recomputes each segment once, saving the momentum of every
+ * step, and runs the adjoint steps over it. grad: double[nx*ny*nz] (0 on
+ * obstacles); *j_out (may be NULL): J of the final state; info (may be NULL,
+ * 6 doubles): forward ms, reverse ms (recomputation + adjoint), interval,
+ * checkpoints, extra device bytes, peak device bytes. The solver's state is
+ * left at the initial state. No counterpart in the reference. */
+int lbm_adjoint_gradient(lbm_solver *s, int steps, int checkpoint_every, double *grad,
+    double *j_out, double *info);
+
 long long lbm_fluid_cells(const lbm_solver *s);
 long long lbm_steps_done(const lbm_solver *s);
 /* Device bytes the solver holds (state, masks, porosity, scratch). */

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include "lbm_adjoint.cuh"
 #include "lbm_step.cuh"
 #include "lbm_step_x2.cuh"
 
@@ -20,6 +21,13 @@ cudaError_t launch_step_x2_f32(int kind, bool force, bool brink, const StepArgs2
     cudaStream_t st);
 cudaError_t launch_step_x2_f16(int kind, bool force, bool brink, const StepArgs2<StoreF16> &a,
     cudaStream_t st);
+
+// Adjoint launchers (lbm_adjoint.cu): one reverse step; seed of lambda at
+// the final state for the outlet objective on device plane x = xo.
+cudaError_t launch_adjoint_step_f64(const AdjArgs<double> &a, cudaStream_t st);
+cudaError_t launch_adjoint_step_f32(const AdjArgs<float> &a, cudaStream_t st);
+cudaError_t launch_adjoint_seed(int precision, const Grid &g, int xo, double inv_count,
+    void *lam, const uint32_t *mask, cudaStream_t st);
 
 // Records the message returned by lbm_last_error() and returns `code`.
 int record_error(int code, const char *fmt, ...);

@@ -17,6 +17,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "lbm_b200.h"
@@ -70,6 +71,7 @@ struct lbm_solver {
   long long launches;
   size_t dev_bytes;
   int no_shuffle; // reduced precision: never use the shuffle-aligned kernels
+  void *u_save_next; // adjoint recomputation: momentum output of the next step
 };
 
 extern "C" const char *lbm_last_error(void) { return g_err; }
@@ -973,7 +975,7 @@ static int launch_one(lbm_solver *s, int *kind_out)
     a.dst = (double *)dst;
     a.mask = s->mask;
     a.porosity = s->porosity;
-    a.u_save = nullptr;
+    a.u_save = brink ? (double *)s->u_save_next : nullptr;
     a.c = make_consts<double>(s);
     e = launch_step_f64(kind, force, brink, a, grid, block, s->stream);
   } else if (s->precision == LBM_F32) {
@@ -983,7 +985,7 @@ static int launch_one(lbm_solver *s, int *kind_out)
     a.dst = (float *)dst;
     a.mask = s->mask;
     a.porosity = s->porosity;
-    a.u_save = nullptr;
+    a.u_save = brink ? (float *)s->u_save_next : nullptr;
     a.c = make_consts2(s);
     a.no_shuffle = s->no_shuffle;
     e = launch_step_x2_f32(kind, force, brink, a, s->stream);
@@ -1233,6 +1235,204 @@ extern "C" int lbm_objective(lbm_solver *s, double *j)
   CUDA_TRY(cudaStreamSynchronize(s->stream));
   *j = h[1] > 0 ? h[0] / h[1] : 0.0;
   return LBM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint of the Brinkman step with checkpointing
+// ---------------------------------------------------------------------------
+
+// Sum of the x momentum and number of fluid cells on the caller's plane
+// x = nx-1.
+static int outlet_sums(lbm_solver *s, double *sum, double *count)
+{
+  if (s->precision == LBM_F64)
+    outlet_launch<StoreF64>(s);
+  else if (s->precision == LBM_F32)
+    outlet_launch<StoreF32>(s);
+  else
+    outlet_launch<StoreF16>(s);
+  CUDA_TRY(cudaGetLastError());
+  double *fin = s->red + (size_t)kRedBlocks * kRedVals;
+  final_reduce_kernel<<<1, kRedThreads, 0, s->stream>>>(s->red, kRedBlocks, 0u, fin);
+  CUDA_TRY(cudaGetLastError());
+  double h[kRedVals];
+  CUDA_TRY(cudaMemcpyAsync(h, fin, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  *sum = h[0];
+  *count = h[1];
+  return LBM_OK;
+}
+
+// per-cell gradient (device cell order) -> caller's dense order
+__global__ void grad_to_dense_kernel(Grid g, UserBox u, const double *__restrict__ grad,
+    const uint32_t *__restrict__ mask, double *dense)
+{
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= u.nz || y >= u.ny)
+    return;
+  const uint32_t cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
+  dense[dense_index(u, x, y, z)] = (mask[cell] & kSolidBit) ? 0.0 : grad[cell];
+}
+
+extern "C" int lbm_adjoint_gradient(lbm_solver *s, int steps, int checkpoint_every,
+    double *grad, double *j_out, double *info)
+{
+  if (!s || steps < 1 || !grad)
+    return fail(LBM_ERR_ARG, "lbm_adjoint_gradient: bad arguments");
+  if (s->pattern != LBM_AA)
+    return fail(LBM_ERR_ARG, "lbm_adjoint_gradient: needs an AA solver");
+  if (s->precision == LBM_F16)
+    return fail(LBM_ERR_ARG, "lbm_adjoint_gradient: FP16 storage is not supported (FP64/FP32)");
+  if (!s->porosity || s->alpha == 0.0)
+    return fail(LBM_ERR_STATE, "lbm_adjoint_gradient: set a porosity field first");
+  CUDA_TRY(cudaSetDevice(s->device));
+  const bool f64 = s->precision == LBM_F64;
+  const size_t vs = f64 ? sizeof(double) : sizeof(float);
+  const size_t P = (size_t)s->g.plane;
+  const size_t ubytes = 3 * P * vs;  // momentum of one step
+  const size_t lbytes = Q * P * vs;  // one adjoint lattice
+  // checkpoint interval: given, or the one that minimises checkpoints
+  // (steps/k states) plus the segment's saved momenta (k momentum sets)
+  int k = checkpoint_every;
+  if (k <= 0) {
+    k = (int)ceil(sqrt((double)steps * (double)s->state_bytes / (double)ubytes));
+    if (k < 1)
+      k = 1;
+  }
+  if (k > steps)
+    k = steps;
+  const int nck = (steps + k - 1) / k;
+  const size_t extra = (size_t)nck * s->state_bytes + (size_t)k * ubytes + 2 * lbytes + P * 8;
+
+  char *ck = NULL, *ub = NULL, *lam = NULL;
+  double *dg = NULL;
+  cudaEvent_t e0 = NULL, e1 = NULL;
+  int rc = LBM_OK;
+#define ATRY(x)                                                                               do {                                                                                          cudaError_t err_ = (x);                                                                     if (err_ != cudaSuccess) {                                                                    rc = fail(err_ == cudaErrorMemoryAllocation ? LBM_ERR_ALLOC : LBM_ERR_CUDA,                    "lbm_adjoint_gradient: %s: %s", #x, cudaGetErrorString(err_));                         goto done;                                                                                }                                                                                         } while (0)
+#define RTRY(x)                                                                               do {                                                                                          rc = (x);                                                                                   if (rc)                                                                                       goto done;                                                                              } while (0)
+  {
+    ATRY(cudaMalloc((void **)&ck, (size_t)nck * s->state_bytes));
+    ATRY(cudaMalloc((void **)&ub, (size_t)k * ubytes));
+    ATRY(cudaMalloc((void **)&lam, 2 * lbytes));
+    ATRY(cudaMalloc((void **)&dg, P * 8));
+    ATRY(cudaEventCreate(&e0));
+    ATRY(cudaEventCreate(&e1));
+    const long long t0 = s->steps_done;
+    void *state = s->buf[0];
+
+    // forward sweep: checkpoint every k steps
+    ATRY(cudaEventRecord(e0, s->stream));
+    for (int c = 0; c < nck; ++c) {
+      ATRY(cudaMemcpyAsync(ck + (size_t)c * s->state_bytes, state, s->state_bytes,
+          cudaMemcpyDeviceToDevice, s->stream));
+      RTRY(lbm_run(s, std::min(k, steps - c * k)));
+    }
+    ATRY(cudaEventRecord(e1, s->stream));
+    ATRY(cudaEventSynchronize(e1));
+    float fwd_ms = 0.f;
+    ATRY(cudaEventElapsedTime(&fwd_ms, e0, e1));
+
+    double jsum = 0.0, jcount = 0.0;
+    RTRY(outlet_sums(s, &jsum, &jcount));
+    if (j_out)
+      *j_out = jcount > 0 ? jsum / jcount : 0.0;
+
+    // reverse sweep
+    ATRY(cudaEventRecord(e0, s->stream));
+    ATRY(launch_adjoint_seed(f64 ? kF64 : kF32, s->g, s->ub.ox + s->ub.nx - 1,
+        jcount > 0 ? 1.0 / jcount : 0.0, lam, s->mask, s->stream));
+    ATRY(cudaMemsetAsync(dg, 0, P * 8, s->stream));
+    int cur = 0; // lambda^{t+1} lives in lam + cur * lbytes
+    float adj_ms = 0.f;
+    for (int c = nck - 1; c >= 0; --c) {
+      const int tc = c * k, len = std::min(k, steps - tc);
+      ATRY(cudaMemcpyAsync(state, ck + (size_t)c * s->state_bytes, s->state_bytes,
+          cudaMemcpyDeviceToDevice, s->stream));
+      s->steps_done = t0 + tc;
+      for (int i = 0; i < len; ++i) {
+        s->u_save_next = ub + (size_t)i * ubytes;
+        rc = launch_one(s, NULL);
+        s->u_save_next = NULL;
+        if (rc)
+          goto done;
+      }
+      for (int i = len - 1; i >= 0; --i) {
+        if (f64) {
+          AdjArgs<double> a;
+          a.g = s->g;
+          a.lam_next = (const double *)(lam + cur * lbytes);
+          a.lam = (double *)(lam + (cur ^ 1) * lbytes);
+          a.u = (const double *)(ub + (size_t)i * ubytes);
+          a.mask = s->mask;
+          a.porosity = s->porosity;
+          a.grad = dg;
+          a.oE = s->omega;
+          a.oO = 1.0 / (0.5 + s->lambda / (1.0 / s->omega - 0.5));
+          a.w0 = 1.0 / 3.0;
+          a.w1 = 1.0 / 18.0;
+          a.w2 = 1.0 / 36.0;
+          a.alpha = s->alpha;
+          ATRY(launch_adjoint_step_f64(a, s->stream));
+        } else {
+          AdjArgs<float> a;
+          a.g = s->g;
+          a.lam_next = (const float *)(lam + cur * lbytes);
+          a.lam = (float *)(lam + (cur ^ 1) * lbytes);
+          a.u = (const float *)(ub + (size_t)i * ubytes);
+          a.mask = s->mask;
+          a.porosity = s->porosity;
+          a.grad = dg;
+          a.oE = (float)s->omega;
+          a.oO = (float)(1.0 / (0.5 + s->lambda / (1.0 / s->omega - 0.5)));
+          a.w0 = (float)(1.0 / 3.0);
+          a.w1 = (float)(1.0 / 18.0);
+          a.w2 = (float)(1.0 / 36.0);
+          a.alpha = (float)s->alpha;
+          ATRY(launch_adjoint_step_f32(a, s->stream));
+        }
+        cur ^= 1;
+      }
+    }
+    ATRY(cudaEventRecord(e1, s->stream));
+    ATRY(cudaEventSynchronize(e1));
+    ATRY(cudaEventElapsedTime(&adj_ms, e0, e1));
+
+    // leave the solver at the initial state
+    ATRY(cudaMemcpyAsync(state, ck, s->state_bytes, cudaMemcpyDeviceToDevice, s->stream));
+    s->steps_done = t0;
+    {
+      dim3 grid, block;
+      user_launch_shape(s, grid, block);
+      grad_to_dense_kernel<<<grid, block, 0, s->stream>>>(s->g, s->ub, dg, s->mask, s->staging);
+      ATRY(cudaGetLastError());
+      ATRY(cudaMemcpyAsync(grad, s->staging, sizeof(double) * (size_t)s->nx * s->ny * s->nz,
+          cudaMemcpyDeviceToHost, s->stream));
+      ATRY(cudaStreamSynchronize(s->stream));
+    }
+    if (info) {
+      info[0] = fwd_ms;
+      info[1] = adj_ms;
+      info[2] = k;
+      info[3] = nck;
+      info[4] = (double)extra;
+      info[5] = (double)(s->dev_bytes + extra);
+    }
+  }
+done:
+  s->u_save_next = NULL;
+  cudaFree(ck);
+  cudaFree(ub);
+  cudaFree(lam);
+  cudaFree(dg);
+  if (e0)
+    cudaEventDestroy(e0);
+  if (e1)
+    cudaEventDestroy(e1);
+#undef ATRY
+#undef RTRY
+  return rc;
 }
 
 extern "C" int lbm_pin_host(void *ptr, size_t bytes)

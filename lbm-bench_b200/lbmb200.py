@@ -64,6 +64,9 @@ _SIGNATURES = [
     ("lbm_mass_momentum_noalloc", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int,
                                                  ctypes.c_int, _dp, _llp, _vp]),
     ("lbm_objective", ctypes.c_int, [_vp, _dp]),
+    ("lbm_adjoint_gradient", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp]),
+    ("lbm_set_state_padded", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int]),
+    ("lbm_get_state_padded", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int]),
     ("lbm_fluid_cells", ctypes.c_longlong, [_vp]),
     ("lbm_steps_done", ctypes.c_longlong, [_vp]),
     ("lbm_device_bytes", ctypes.c_size_t, [_vp]),
@@ -224,6 +227,18 @@ class Solver:
         j = ctypes.c_double(0.0)
         _check(lib().lbm_objective(self._h, ctypes.byref(j)))
         return j.value
+
+    def adjoint_gradient(self, steps: int, checkpoint_every: int = 0):
+        """dJ/dphi after `steps` Brinkman steps from the current state
+        (lbm_adjoint_gradient). Returns (J, grad[nx, ny, nz], info dict)."""
+        grad = np.zeros(self.shape)
+        j = ctypes.c_double(0.0)
+        info = np.zeros(6)
+        _check(lib().lbm_adjoint_gradient(self._h, int(steps), int(checkpoint_every),
+                                          _p(grad, _dp), ctypes.byref(j), _p(info, _dp)))
+        keys = ("forward_ms", "reverse_ms", "interval", "checkpoints", "extra_bytes",
+                "peak_bytes")
+        return j.value, grad, dict(zip(keys, info.tolist()))
 
     @property
     def fluid_cells(self) -> int:
