@@ -18,12 +18,30 @@ and the download of the final state, all inside the timed region.
 Variants: FP64 pull and push, FP32 and FP16 storage (FP32 arithmetic) with
 their L2 velocity/density error against the FP64 run of the same seed.
 
+Adjoint (`adjoint` key of the default line): 128^3 Brinkman channel (walls
+on the y and z faces, x periodic, FP32 porosity uniform in [0, 1] from a
+seed, Brinkman coefficient kappa = 0.1 (1 - phi)), J = mean x velocity on the
+outlet plane after 2000 steps, checkpoints every 100 steps; seconds per
+step and cost in forward steps, the FP64 gradient against FP64 central
+finite differences (eps = 1e-4) at 20 seeded fluid cells, and the FP32
+gradient against the FP64 one.
+
+Other workloads, one JSON line each (`--config`):
+  2  precision study: 512^3 porous channel (20% solid, r 4-8), 300 steps,
+     FP32 and FP16 storage against the FP64 run of the same seed
+  3  the adjoint study alone
+  4  largest single-GPU sizes: 768^3 porous channel (30% solid, r 6-12),
+     FP16 storage, AA, 200 steps; the 384^3 Brinkman adjoint, 1000 steps,
+     sqrt checkpoint schedule; peak device memory against the 180 GB HBM
+
 `--impl reference` times LBM-Bench's own CPU kernels (compiled from the
 reference sources into oracle/_ref) on the host cores on the same workload.
 
-Multi-GPU (`--gpus N` under torchrun): each rank runs an independent replica
-of the workload on its own GPU (weak scaling); value = all ranks' updates /
-max rank time.
+Multi-GPU (`--gpus N` under torchrun): the porous channel grows to
+(N x 256) x 256 x 256 and is cut into one 256^3 x-slab per rank (weak
+scaling); each odd AA step exchanges the five x-crossing populations of the
+slab faces with the ring neighbours over NCCL (lbm_slab); value = all
+ranks' fluid updates / max rank device time.
 """
 from __future__ import annotations
 
@@ -155,10 +173,16 @@ class Dist:
             self.dist.barrier()
 
     def max(self, v: float) -> float:
+        return self._reduce(v, "MAX")
+
+    def sum(self, v: float) -> float:
+        return self._reduce(v, "SUM")
+
+    def _reduce(self, v: float, op: str) -> float:
         if not self.pg:
             return v
         t = self.torch.tensor([v], dtype=self.torch.float64, device="cuda")
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        self.dist.all_reduce(t, op=getattr(self.dist.ReduceOp, op))
         return float(t.item())
 
     def close(self):
@@ -229,6 +253,8 @@ def run_native(args, dist: Dist):
 
     if L.device_count() <= 0:
         raise SystemExit("bench.py: no CUDA device; the native arm has no CPU path")
+    if dist.world > 1:
+        return run_slabs(args, dist)
     n = args.size
     flags, f0, frac, nsph = make_workload(L, n)
     peak, peak_kind = measured_hbm_peak()
@@ -296,6 +322,9 @@ def run_native(args, dist: Dist):
     # ---- e2e: through the reference-facing call with pinned host buffers
     e2e = run_e2e(L, flags, f0, args.steps, dist)
 
+    # ---- adjoint of the Brinkman step (128^3, 2000 steps, checkpoints every 100)
+    adjoint = adjoint_study(L, 128, 2000, 100, 20) if not args.no_adjoint else None
+
     result = {
         "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": dist.world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -305,7 +334,7 @@ def run_native(args, dist: Dist):
                        fluid_cells=n_fluid, parallelism=f"replicas x{dist.world}"),
         "gbs": n_fluid * bpu * args.steps / (ms / 1e3) / 1e9,
         "roofline": roofline, "e2e": e2e, "gpu_launches": launches,
-        "clocks": clk.summary(), "variants": variants,
+        "clocks": clk.summary(), "variants": variants, "adjoint": adjoint,
         "state_check": {"mass": tot[0], "nonfinite_cells": bad},
         "device_bytes": s.device_bytes,
     }
@@ -320,6 +349,308 @@ def run_native(args, dist: Dist):
         except Exception as exc:  # reported, not fatal
             result["cpu_baseline"] = {"value": None, "unit": "MLUPS", "error": str(exc)}
     return result
+
+
+# ---------------------------------------------------------------------------
+# adjoint of the Brinkman step
+# ---------------------------------------------------------------------------
+
+ADJ = {"omega": 1.25, "lambda": 3 / 16, "xforce": 1e-6, "alpha": 0.1, "porosity_seed": 11,
+       "init_seed": 7, "amplitude": 1e-4}
+
+
+def adjoint_solver(L, flags, por, precision):
+    s = L.Solver(flags, (1, 0, 0), "aa", precision)
+    s.set_params(ADJ["omega"], ADJ["lambda"], ADJ["xforce"], True)
+    s.set_porosity(por, ADJ["alpha"])
+    s.init_equilibrium(seed=ADJ["init_seed"], amplitude=ADJ["amplitude"])
+    return s
+
+
+def adjoint_study(L, n: int, steps: int, ckpt: int, fd_cells: int, precisions=("fp64", "fp32")):
+    """Gradient of J = mean outlet-plane u_x after `steps` Brinkman steps
+    with respect to the porosity field: time per step, cost in forward
+    steps, FD check (FP64, central, eps 1e-4) and FP32 vs FP64."""
+    import numpy as np
+
+    dims = (n, n, n)
+    flags, _, _ = L.geometry("channel", dims)
+    rng = np.random.default_rng(ADJ["porosity_seed"])
+    por = rng.uniform(0.0, 1.0, size=dims).astype(np.float32)
+    fluid = np.transpose(flags, (2, 1, 0)) != 0
+    prec = {"fp64": L.F64, "fp32": L.F32}
+    out = {"workload": f"Brinkman channel {n}^3, porosity U[0,1] seed {ADJ['porosity_seed']}",
+           "dims": list(dims), "steps": steps, "checkpoint_every": ckpt,
+           "objective": "mean u_x over the fluid cells of the outlet plane x = nx-1",
+           **{k: ADJ[k] for k in ("omega", "lambda", "xforce", "alpha")}}
+    grads = {}
+    for name in precisions:
+        s = adjoint_solver(L, flags, por, prec[name])
+        n_fluid = s.fluid_cells
+        s.run(5)
+        fwd_ms = s.run_timed(steps) / steps  # plain Brinkman forward step
+        s.init_equilibrium(seed=ADJ["init_seed"], amplitude=ADJ["amplitude"])
+        j, g, info = s.adjoint_gradient(steps, ckpt)
+        total_ms = info["forward_ms"] + info["reverse_ms"]
+        grads[name] = g
+        out[name] = {
+            "J": j, "s_per_step": total_ms / 1e3 / steps,
+            "forward_step_ms": fwd_ms,
+            "cost_in_forward_steps": total_ms / steps / fwd_ms,
+            "reverse_cost_in_forward_steps": info["reverse_ms"] / steps / fwd_ms,
+            "forward_sweep_ms": info["forward_ms"], "reverse_sweep_ms": info["reverse_ms"],
+            "checkpoint_interval": int(info["interval"]), "checkpoints": int(info["checkpoints"]),
+            "peak_device_bytes": int(info["peak_bytes"]),
+            "forward_mlups": n_fluid / fwd_ms / 1e3}
+        if name == "fp64" and fd_cells:
+            out["fd_check"] = finite_differences(s, por, g, fluid, steps, fd_cells)
+        if name == "fp64" and ckpt > 0:
+            # the same gradient with the least recomputation that fits in memory
+            s.init_equilibrium(seed=ADJ["init_seed"], amplitude=ADJ["amplitude"])
+            _, ga, ia = s.adjoint_gradient(steps, L.CKPT_AUTO)
+            ta = ia["forward_ms"] + ia["reverse_ms"]
+            out["fp64_auto_schedule"] = {
+                "s_per_step": ta / 1e3 / steps, "cost_in_forward_steps": ta / steps / fwd_ms,
+                "reverse_cost_in_forward_steps": ia["reverse_ms"] / steps / fwd_ms,
+                "checkpoint_interval": int(ia["interval"]), "checkpoints": int(ia["checkpoints"]),
+                "peak_device_bytes": int(ia["peak_bytes"]),
+                "gradient_bitwise_equal_to_interval_run": bool(np.array_equal(ga, g))}
+        s.close()
+    if "fp64" in grads and "fp32" in grads:
+        a, b = grads["fp64"], grads["fp32"]
+        out["fp32_vs_fp64_grad_l2_rel"] = float(np.linalg.norm(b - a) / np.linalg.norm(a))
+    return out
+
+
+def finite_differences(s, por, g, fluid, steps, ncells, eps=1e-4, h=5e-3, seed=2024):
+    """FP64 central differences of J at `ncells` seeded fluid cells, on the
+    solver `s` (its porosity is restored afterwards): with step `eps`, and
+    Richardson-extrapolated from steps h and 2h, (4 D(h) - D(2h)) / 3,
+    whose truncation error is O(h^4) and whose round-off floor is eps/h
+    times lower. The round-off of J (about 1e-18 absolute here, against
+    differences 2 eps dJ/dphi of about 4e-15) is what limits the eps = 1e-4
+    quotient far from the outlet."""
+    import numpy as np
+
+    def j_at(c, delta):
+        p = por.copy()
+        p[c] = np.float32(p[c] + delta)
+        s.set_porosity(p, ADJ["alpha"])
+        s.init_equilibrium(seed=ADJ["init_seed"], amplitude=ADJ["amplitude"])
+        s.run(steps)
+        return float(p[c]), s.objective()
+
+    def quotient(c, step):
+        (pa, ja), (pb, jb) = j_at(c, step), j_at(c, -step)
+        return (ja - jb) / (pa - pb)
+
+    rng = np.random.default_rng(seed)
+    cells = np.argwhere(fluid)
+    picks = [tuple(int(v) for v in cells[i])
+             for i in rng.choice(len(cells), ncells, replace=False)]
+    rows = []
+    for c in picks:
+        fd = quotient(c, eps)
+        rich = (4.0 * quotient(c, h) - quotient(c, 2 * h)) / 3.0
+        gc = float(g[c])
+        rows.append({"cell": list(c), "adjoint": gc, "fd": fd, "fd_richardson": rich,
+                     "rel_err": abs(gc - fd) / abs(fd), "rel_err_richardson":
+                     abs(gc - rich) / abs(rich)})
+    s.set_porosity(por, ADJ["alpha"])
+    gv = np.array([r["adjoint"] for r in rows])
+    out = {"cells": ncells, "seed": seed, "per_cell": rows}
+    for key, name in (("fd", f"eps_{eps:g}"), ("fd_richardson", f"richardson_h_{h:g}")):
+        errs = np.array([r["rel_err" if key == "fd" else "rel_err_richardson"] for r in rows])
+        fv = np.array([r[key] for r in rows])
+        out[name] = {"max_rel_err": float(errs.max()), "median_rel_err": float(np.median(errs)),
+                     "cells_within_1e-4": int((errs <= 1e-4).sum()),
+                     "normwise_rel_err": float(np.linalg.norm(gv - fv) / np.linalg.norm(fv))}
+    return out
+
+
+# ---------------------------------------------------------------------------
+# other workloads (--config 2, 3, 4)
+# ---------------------------------------------------------------------------
+
+def base_line(metric_value, unit, steps, warmup, ms, workload, dtype, extra):
+    r = {"metric": METRIC, "value": metric_value, "unit": unit, "n_gpus": 1, "steps": steps,
+         "warmup": warmup, "ms_per_step": ms, "higher_is_better": unit != "s/step",
+         "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+         "data": "synthetic (seeded porous geometry and initial state)", "config": workload}
+    r.update(extra)
+    return r
+
+
+def timed_forward(L, flags, pattern, precision, steps, warmup, peak):
+    s = L.Solver(flags, (1, 0, 0), pattern, precision)
+    s.set_params(1.25, 3 / 16, 1e-6, True)
+    s.init_equilibrium(seed=7, amplitude=1e-4)
+    s.run(warmup)
+    with ClockSampler(0) as clk:
+        ms = s.run_timed(steps)
+    n_fluid = s.fluid_cells
+    mlups = n_fluid * steps / (ms / 1e3) / 1e6
+    gbs = mlups * s.bytes_per_update / 1e3
+    return s, {"mlups": mlups, "gbs": gbs, "frac": gbs / peak, "ms_per_step": ms / steps,
+               "fluid_cells": n_fluid, "device_bytes": s.device_bytes,
+               "bytes_per_update": s.bytes_per_update, "clocks": clk.summary()}
+
+
+def run_precision_study(args):
+    """512^3 porous channel, 300 steps: FP32 and FP16 storage of f - w
+    (FP32 arithmetic) against the FP64 run of the same seed."""
+    import lbmb200 as L
+    import numpy as np
+
+    n, steps = args.size or 512, args.steps
+    flags, frac, nsph = L.porous_channel((n, n, n), 0.2, 4.0, 8.0, seed=42)
+    peak, peak_kind = measured_hbm_peak()
+    ref, r64 = timed_forward(L, flags, "aa", L.F64, steps, 0, peak)
+    res = {"fp64_aa": r64}
+    for name, prec in (("fp32", L.F32), ("fp16", L.F16)):
+        b, r = timed_forward(L, flags, "aa", prec, steps, 0, peak)
+        d = b.compare(ref)
+        r["l2_rel_err_u"] = float(np.sqrt(d[0] / d[1])) if d[1] > 0 else None
+        r["l2_rel_err_rho"] = float(np.sqrt(d[2] / d[3])) if d[3] > 0 else None
+        r["speedup_vs_fp64_aa"] = r["mlups"] / r64["mlups"]
+        res[f"{name}_aa"] = r
+        b.close()
+    tot, bad = ref.mass_momentum(check=False)
+    ref.close()
+    wl = {"workload": f"precision study, porous channel {n}^3, 20% solid spheres r 4-8, seed 42",
+          "dims": [n] * 3, "solid_fraction_achieved": frac, "spheres": nsph,
+          "steps": steps, "omega": 1.25, "lambda": 3 / 16, "xforce": 1e-6,
+          "init": "equilibrium +-1e-4 seed 7 (generated on the device)",
+          "error": "L2 relative error of u and rho over fluid cells vs the FP64 run after "
+                   f"{steps} steps", "hbm_peak_gbs": peak, "hbm_peak_source": peak_kind,
+          "l2_flush": "not needed: states of 5-20 GB > 126 MB L2"}
+    f16 = res["fp16_aa"]
+    return base_line(f16["mlups"], "MLUPS", steps, 0, f16["ms_per_step"], wl, "f32 (f16 storage)",
+                     {"variants": res, "fp64_nonfinite_cells": bad})
+
+
+def run_adjoint_only(args):
+    import lbmb200 as L
+    a = adjoint_study(L, args.size or 128, args.steps, 100, 20)
+    return base_line(a["fp64"]["s_per_step"], "s/step", args.steps, 5,
+                     a["fp64"]["s_per_step"] * 1e3, {"workload": a["workload"]}, "f64",
+                     {"adjoint": a})
+
+
+def run_largest(args):
+    """768^3 FP16 forward (30% solid, r 6-12, 200 steps) and the 384^3
+    FP32 Brinkman adjoint with the sqrt checkpoint schedule (1000 steps)."""
+    import lbmb200 as L
+
+    n = args.size or 768
+    peak, peak_kind = measured_hbm_peak()
+    flags, frac, nsph = L.porous_channel((n, n, n), 0.3, 6.0, 12.0, seed=42)
+    free0, total = L.device_memory()
+    s, fwd = timed_forward(L, flags, "aa", L.F16, args.steps, 3, peak)
+    free1, _ = L.device_memory()
+    tot, bad = s.mass_momentum(check=False)
+    fwd.update({"nonfinite_cells": bad, "device_used_bytes": total - free1,
+                "device_total_bytes": total, "solid_fraction_achieved": frac, "spheres": nsph})
+    s.close()
+    del flags
+    na = 384
+    a = adjoint_study(L, na, 1000, 0, 0, precisions=("fp32",))
+    a["fp32"]["device_total_bytes"] = total
+    wl = {"workload": f"largest single-GPU sizes: FP16 porous channel {n}^3 (30% solid, r 6-12), "
+                      f"{args.steps} steps; FP32 Brinkman adjoint {na}^3, 1000 steps, sqrt "
+                      "checkpoint schedule",
+          "hbm_peak_gbs": peak, "hbm_peak_source": peak_kind, "hbm_capacity_gb": 180}
+    return base_line(fwd["mlups"], "MLUPS", args.steps, 3, fwd["ms_per_step"], wl,
+                     "f32 (f16 storage)", {"forward_fp16_aa": fwd, "adjoint": a})
+
+
+def run_slabs(args, dist: Dist):
+    """N GPUs: the porous channel of N x 256 x 256 x 256 cells cut into one
+    256^3 x-slab per rank (weak scaling), FP64 AA, halo exchange between
+    ring neighbours over NCCL every odd step (lbm_slab)."""
+    import lbm_slab
+    import lbmb200 as L
+    import numpy as np
+    import torch
+
+    n, world, rank = args.size, dist.world, dist.rank
+    flags, frac, nsph = L.porous_channel((n * world, n, n), 0.2, 4.0, 8.0, seed=42)
+    x0, x1 = lbm_slab.split(n * world, world, rank)
+    sflags = lbm_slab.slab_flags(flags, x0, x1)
+    del flags
+    own = np.ascontiguousarray(sflags[:, :, 1:-1])
+    f0 = L.perturbed_equilibrium(own, seed=7, amplitude=1e-4)
+    peak, peak_kind = measured_hbm_peak()
+
+    s = L.Solver.slab(sflags, (0, 0), "aa", L.F64)
+    s.set_params(1.25, 3 / 16, 1e-6, True)
+    s.set_state(f0)
+    runner = lbm_slab.SlabRunner(s, lbm_slab.Ring())
+    runner.scatter()
+    n_fluid = s.fluid_cells
+    bpu = s.bytes_per_update
+    runner.run(args.warmup)
+    s.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0, ex0 = s.launch_count, runner.exchanges
+    dist.barrier()
+    s.synchronize()
+    with ClockSampler(dist.local) as clk:
+        ev0.record(runner.ext)
+        runner.run(args.steps)
+        ev1.record(runner.ext)
+        ev1.synchronize()
+    dist.barrier()
+    ms = dist.max(ev0.elapsed_time(ev1))
+    total_fluid = dist.sum(float(n_fluid))
+    launches = (s.launch_count - launches0) + 4 * (runner.exchanges - ex0)
+    runner.gather()
+    tot, bad = s.mass_momentum(check=False)
+    mass = dist.sum(tot[0])
+    value = total_fluid * args.steps / (ms / 1e3) / 1e6
+    achieved = n_fluid * bpu * args.steps / (ms / 1e3) / 1e9
+
+    # e2e: the state up from pinned host memory, the steps with their
+    # exchanges, the state back down - host clock, max over ranks
+    host = np.empty_like(f0)
+    L.pin(f0)
+    L.pin(host)
+    dist.barrier()
+    t0 = time.perf_counter()
+    s.set_state(f0)
+    runner.scatter()
+    runner.run(args.steps)
+    runner.gather()
+    s.get_state(out=host)
+    t = dist.max(time.perf_counter() - t0)
+    L.unpin(f0)
+    L.unpin(host)
+    e2e = {"value": total_fluid * args.steps / t / 1e6, "unit": "MLUPS",
+           "h2d_bytes_per_step": f0.nbytes / args.steps,
+           "d2h_bytes_per_step": host.nbytes / args.steps, "seconds": t,
+           "call": "lbm_set_state (pinned host) + SlabRunner.run (steps + NCCL halo exchange) + "
+                   "lbm_get_state, per rank"}
+    s.close()
+    return {
+        "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded porous geometry and initial state)",
+        "config": dict(WORKLOAD, workload=f"porous channel {n * world}x{n}x{n} (one {n}^3 x-slab "
+                                          "per GPU), 20% solid spheres r 4-8, seed 42",
+                       dims=[n * world, n, n], solid_fraction_achieved=frac, spheres=nsph,
+                       fluid_cells=int(total_fluid), parallelism=f"x-slabs x{world}",
+                       halo="5 populations x 256 x 256 per face, before and after each odd "
+                            "AA step, NCCL send/recv between ring neighbours"),
+        "gbs": achieved * world,
+        "roofline": {"bound": "hbm", "kernel": "step_kernel<StoreF64> AA even+odd with halo "
+                                               "exchange (whole step, per GPU)",
+                     "achieved": achieved, "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "algorithmic_bytes_per_launch": n_fluid * bpu},
+        "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
+        "state_check": {"mass": mass, "nonfinite_cells_rank0": bad},
+    }
 
 
 def run_e2e(L, flags, f0, steps, dist: Dist):
@@ -388,9 +719,24 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--config", type=int, choices=[1, 2, 3, 4], default=1,
+                    help="1: 256^3 patterns (default); 2: 512^3 precision study; "
+                         "3: 128^3 adjoint; 4: 768^3 FP16 and 384^3 adjoint")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.config != 1:
+        if args.impl == "reference" or args.gpus != 1:
+            ap.error("--config 2-4 run the native arm on one GPU")
+        defaults = {2: 300, 3: 2000, 4: 200}
+        if "--steps" not in sys.argv:
+            args.steps = defaults[args.config]
+        if "--size" not in sys.argv:
+            args.size = None
+        fn = {2: run_precision_study, 3: run_adjoint_only, 4: run_largest}[args.config]
+        print(json.dumps(fn(args)), flush=True)
+        return
     if args.impl == "reference":
         res = run_reference(args)
         if res is not None:

@@ -62,6 +62,16 @@ typedef struct lbm_solver lbm_solver;
 int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *flags, int periodic_x,
     int periodic_y, int periodic_z, int pattern, int precision);
 
+/* One x-slab of a domain decomposed along x (x is the slowest axis of the
+ * reference's indexSoA, src/lbm.h:113-116). `flags` holds nx + 2 planes in
+ * x (x fastest): planes 0 and nx + 1 are the boundary planes of the left and
+ * right neighbouring slabs (periodic wrap at the ends of the ring). They
+ * become ghost planes: never updated here, filled and drained through the
+ * halo functions below. y and z are as in lbm_create. No counterpart in the
+ * reference (single-node OpenMP only). */
+int lbm_create_slab(lbm_solver **out, int nx, int ny, int nz, const int *flags, int periodic_y,
+    int periodic_z, int pattern, int precision);
+
 /* Frees everything the solver owns (src/lbm.c:660-670). NULL is a no-op. */
 int lbm_destroy(lbm_solver *s);
 
@@ -106,6 +116,39 @@ int lbm_get_state(lbm_solver *s, double *f);
  * Replaces the host-side SetNode/GetNode loops around a kd->Kernel call. */
 int lbm_set_state_padded(lbm_solver *s, const void *pdfs, int elem_size, int ref_orientation);
 int lbm_get_state_padded(lbm_solver *s, void *pdfs, int elem_size, int ref_orientation);
+
+/* Halo exchange of slab solvers. lbm_halo_needs tells which exchanges the
+ * next step takes (LBM_HALO_BEFORE: pull, AA odd; LBM_HALO_AFTER: push, AA
+ * odd; none for an AA even step). lbm_halo_pack writes the two messages
+ * (lbm_halo_bytes each) into device buffers, to_left for the left
+ * neighbour and to_right for the right one; after the transport,
+ * lbm_halo_unpack reads what the left and right neighbours sent. Both are
+ * ordered on the solver's stream (lbm_stream). `when` is LBM_HALO_BEFORE
+ * (before lbm_run(s, 1)) or LBM_HALO_AFTER (after it). */
+#define LBM_HALO_BEFORE 1
+#define LBM_HALO_AFTER 2
+/* The pull state, and the AA state after an odd number of steps, keep
+ * populations of a slab's boundary cells in the ghost planes
+ * (lbm_halo_shifted returns 1). Then a LBM_HALO_BEFORE exchange must come
+ * before reading the state (lbm_get_state, lbm_moments, lbm_mass_momentum,
+ * lbm_compare), and a LBM_HALO_SCATTER exchange after lbm_set_state, which
+ * sends those ghost slots to the neighbours' own planes. */
+#define LBM_HALO_SCATTER 4
+size_t lbm_halo_bytes(const lbm_solver *s);
+int lbm_halo_needs(const lbm_solver *s);
+int lbm_halo_shifted(const lbm_solver *s);
+int lbm_halo_pack(lbm_solver *s, int when, void *to_left, void *to_right);
+int lbm_halo_unpack(lbm_solver *s, int when, const void *from_left, const void *from_right);
+/* The solver's CUDA stream (cudaStream_t), for ordering a transport on it. */
+void *lbm_stream(const lbm_solver *s);
+
+/* Sets the state on the device to the seeded initial condition of
+ * lbm_perturbed_equilibrium (identical values, no host array): for domains
+ * whose FP64 host state would not fit in host memory. */
+int lbm_init_equilibrium(lbm_solver *s, unsigned long long seed, double amplitude, double rho);
+
+/* Free and total memory of the current CUDA device (cudaMemGetInfo). */
+int lbm_device_memory(size_t *free_bytes, size_t *total_bytes);
 
 /* Enqueues `steps` time steps on the solver's stream (asynchronous).
  * Replaces the time loop of kd->Kernel (src/kernel_pull_soa.c:44-214,
@@ -181,13 +224,17 @@ int lbm_objective(lbm_solver *s, double *j);
  * of the step, reverse in time. AA solvers with FP64 or FP32 storage and a
  * porosity field set (lbm_set_porosity). The forward sweep keeps a
  * checkpoint every `checkpoint_every` steps (0: the interval that minimises
- * checkpoint plus segment memory, about sqrt(steps * state / momentum)); the
- * reverse sweep recomputes each segment once, saving the momentum of every
- * step, and runs the adjoint steps over it. grad: double[nx*ny*nz] (0 on
+ * checkpoint plus segment memory, about sqrt(steps * state / momentum);
+ * LBM_CKPT_AUTO: the longest interval that fits in 90% of the free device
+ * memory, up to `steps`, i.e. the least recomputation); the reverse sweep
+ * recomputes each segment but the last once, saving the momentum of every
+ * step (the forward sweep saves the last segment's), and runs the adjoint
+ * steps over it. grad: double[nx*ny*nz] (0 on
  * obstacles); *j_out (may be NULL): J of the final state; info (may be NULL,
  * 6 doubles): forward ms, reverse ms (recomputation + adjoint), interval,
  * checkpoints, extra device bytes, peak device bytes. The solver's state is
  * left at the initial state. No counterpart in the reference. */
+#define LBM_CKPT_AUTO (-1)
 int lbm_adjoint_gradient(lbm_solver *s, int steps, int checkpoint_every, double *grad,
     double *j_out, double *info);
 

@@ -7,7 +7,7 @@
  * (src/lbm.c:193-294). The functions below have exactly those signatures, so
  * a maintainer adds rows such as
  *     { "cuda-aa-soa", kernelInitCudaAaSoA, kernelDeinitCuda },
- * to GKernels[] and links liblbmb200 (INTEGRATION.md).
+ * to GKernels[] and links liblbmb200.
  *
  * The kernel data the Init functions return keeps the reference's host
  * arrays (Pdfs[0..1] in the padded indexSoA layout, page-locked) and

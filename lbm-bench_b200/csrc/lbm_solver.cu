@@ -72,6 +72,7 @@ struct lbm_solver {
   size_t dev_bytes;
   int no_shuffle; // reduced precision: never use the shuffle-aligned kernels
   void *u_save_next; // adjoint recomputation: momentum output of the next step
+  int slab;          // x-slab of a decomposed domain: device planes 0 and nx+1 are ghosts
 };
 
 extern "C" const char *lbm_last_error(void) { return g_err; }
@@ -169,7 +170,10 @@ static Consts2 make_consts2(const lbm_solver *s)
 
 // One thread per device cell (z < pz): fluid cells get their link mask,
 // every other cell (obstacle, frame, row padding) the wall bit.
-__global__ void mask_kernel(Grid g, const uint8_t *fluid, uint32_t *mask)
+// With ghost_x the planes x = 0 and x = nx-1 hold the neighbouring slabs'
+// boundary cells: they are never updated here (wall bit), but the links of
+// this slab's cells toward them follow their real flags.
+__global__ void mask_kernel(Grid g, const uint8_t *fluid, uint32_t *mask, int ghost_x)
 {
   const int z = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -177,7 +181,7 @@ __global__ void mask_kernel(Grid g, const uint8_t *fluid, uint32_t *mask)
   if (z >= g.pz || y >= g.ny)
     return;
   const uint32_t cell = cell_index(g, x, y, z);
-  if (z >= g.nz || !fluid[cell]) {
+  if (z >= g.nz || !fluid[cell] || (ghost_x && (x == 0 || x == g.nx - 1))) {
     mask[cell] = kSolidBit;
     return;
   }
@@ -507,8 +511,10 @@ static int dev_alloc(lbm_solver *s, void **p, size_t bytes, const char *what)
 // C ABI
 // ---------------------------------------------------------------------------
 
-extern "C" int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *flags,
-    int periodic_x, int periodic_y, int periodic_z, int pattern, int precision)
+// slab = 1: flags has nx + 2 planes in x (x fastest); planes 0 and nx + 1
+// are the neighbouring slabs' boundary planes and become ghost planes.
+static int create_impl(lbm_solver **out, int nx, int ny, int nz, const int *flags,
+    int periodic_x, int periodic_y, int periodic_z, int pattern, int precision, int slab)
 {
   if (!out)
     return fail(LBM_ERR_ARG, "lbm_create: out is NULL");
@@ -529,7 +535,8 @@ extern "C" int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *f
   s->nx = nx;
   s->ny = ny;
   s->nz = nz;
-  s->periodic[0] = periodic_x ? 1 : 0;
+  s->slab = slab;
+  s->periodic[0] = periodic_x && !slab ? 1 : 0;
   s->periodic[1] = periodic_y ? 1 : 0;
   s->periodic[2] = periodic_z ? 1 : 0;
   s->pattern = pattern;
@@ -550,19 +557,22 @@ extern "C" int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *f
   // a non-periodic axis whose faces hold fluid gets a one-cell solid frame
   int frame[3] = { 0, 0, 0 };
   const int dims[3] = { nx, ny, nz };
-  for (int a = 0; a < 3; ++a) {
+  const int fx = nx + 2 * slab; // x extent of the flags array
+  for (int a = slab ? 1 : 0; a < 3; ++a) {
     if (s->periodic[a])
       continue;
     for (int x = 0; x < nx && !frame[a]; ++x)
       for (int y = 0; y < ny && !frame[a]; ++y)
         for (int z = 0; z < nz; ++z) {
           const int c[3] = { x, y, z };
-          if ((c[a] == 0 || c[a] == dims[a] - 1) && flags[((long long)z * ny + y) * nx + x]) {
+          if ((c[a] == 0 || c[a] == dims[a] - 1) && flags[((long long)z * ny + y) * fx + x + slab]) {
             frame[a] = 1;
             break;
           }
         }
   }
+  if (slab)
+    frame[0] = 1; // the ghost planes take the place of an x frame
   s->ub.ox = frame[0];
   s->ub.oy = frame[1];
   s->ub.oz = frame[2];
@@ -623,12 +633,13 @@ extern "C" int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *f
   // fluid bytes in device cell order (frames and padding = wall), then the masks
   std::vector<uint8_t> fluid((size_t)cells, 0);
   long long nf = 0;
-  for (int x = 0; x < nx; ++x)
+  for (int x = -slab; x < nx + slab; ++x)
     for (int y = 0; y < ny; ++y)
       for (int z = 0; z < nz; ++z) {
-        uint8_t f = flags[((long long)z * ny + y) * nx + x] != 0;
+        uint8_t f = flags[((long long)z * ny + y) * fx + x + slab] != 0;
         fluid[((size_t)(x + frame[0]) * s->g.ny + (y + frame[1])) * s->g.pz + z + frame[2]] = f;
-        nf += f;
+        if (x >= 0 && x < nx)
+          nf += f;
       }
   s->n_fluid = nf;
   uint8_t *dfluid = NULL;
@@ -640,7 +651,7 @@ extern "C" int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *f
     gp.nz = s->g.pz; // cover the row padding too
     dim3 grid, block;
     cell_launch_shape(gp, grid, block);
-    mask_kernel<<<grid, block, 0, s->stream>>>(s->g, dfluid, s->mask);
+    mask_kernel<<<grid, block, 0, s->stream>>>(s->g, dfluid, s->mask, s->slab);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess)
@@ -660,6 +671,19 @@ extern "C" int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *f
 #undef TRYC
   *out = s;
   return LBM_OK;
+}
+
+extern "C" int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *flags,
+    int periodic_x, int periodic_y, int periodic_z, int pattern, int precision)
+{
+  return create_impl(out, nx, ny, nz, flags, periodic_x, periodic_y, periodic_z, pattern,
+      precision, 0);
+}
+
+extern "C" int lbm_create_slab(lbm_solver **out, int nx, int ny, int nz, const int *flags,
+    int periodic_y, int periodic_z, int pattern, int precision)
+{
+  return create_impl(out, nx, ny, nz, flags, 0, periodic_y, periodic_z, pattern, precision, 1);
 }
 
 extern "C" int lbm_destroy(lbm_solver *s)
@@ -1238,6 +1262,298 @@ extern "C" int lbm_objective(lbm_solver *s, double *j)
 }
 
 // ---------------------------------------------------------------------------
+// Halo exchange of x-slabs
+// ---------------------------------------------------------------------------
+//
+// A slab's step reads or writes, across each x face, only the five
+// populations with c_x = +1 (set P) or c_x = -1 (set M). Which slots of
+// which plane move, per propagation pattern:
+//   before a pull step   own last plane P -> right ghost, own first plane M -> left ghost
+//   before an AA odd step own last plane M -> right ghost, own first plane P -> left ghost
+//   after a push or AA odd step  right ghost P -> own first plane of the
+//                                right slab, left ghost M -> own last plane of the left slab,
+//                                only into slots that arrived over a fluid link
+// (pull gathers slot d of x - c_d; the AA odd step reads slot inv d of
+// x - c_d and writes slot d of x + c_d; push writes slot d of x + c_d.)
+// AA even steps and push's reads are local. A message is 5 slots x ny x nz
+// storage elements in the caller's y-z order.
+//
+// The pull state and the AA state after an odd number of steps keep some
+// populations of a boundary cell in the neighbouring cell (slot d of
+// x - c_d, or slot inv d of x - c_d), i.e. in a ghost plane: exactly the
+// before-step slot sets. So a before-step exchange also makes such a state
+// readable (lbm_get_state, moments), and LBM_HALO_SCATTER sends what
+// lbm_set_state wrote into the ghost planes to the neighbours' own planes.
+
+// k-th direction (0..4) with c_x == sgn
+__device__ __forceinline__ int halo_dir(int sgn, int k)
+{
+  int n = 0;
+#pragma unroll
+  for (int d = 0; d < Q; ++d)
+    if (cx(d) == sgn) {
+      if (n == k)
+        return d;
+      ++n;
+    }
+  return 0;
+}
+
+// to_buf: state -> message; else message -> state. guard (unpacks into own
+// planes): slot d of a cell is written only if the cell is fluid and the
+// link the slot's population uses is fluid - mask bit inv d (kGuardInv:
+// the population arrived from x - c_d, after a push or AA odd step) or bit
+// d (kGuardOwn: the pull state keeps x + c_d's population d there). Across a
+// wall the cell itself keeps a bounced population in that slot, and the
+// neighbour's ghost slot holds nothing.
+enum HaloGuard { kGuardNone = 0, kGuardInv = 1, kGuardOwn = 2 };
+
+template <typename T>
+__global__ void halo_copy_kernel(Grid g, UserBox u, int xplane, int sgn, T *state, T *buf,
+    int to_buf, const uint32_t *__restrict__ mask, int guarded)
+{
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (z >= u.nz || y >= u.ny)
+    return;
+  const int d = halo_dir(sgn, k);
+  const uint32_t cell = cell_index(g, xplane, y + u.oy, z + u.oz);
+  const size_t si = (size_t)d * g.plane + cell;
+  const size_t bi = ((size_t)k * u.ny + y) * u.nz + z;
+  if (to_buf) {
+    buf[bi] = state[si];
+    return;
+  }
+  if (guarded && (mask[cell] & (kSolidBit | (1u << (guarded == kGuardInv ? inv(d) : d)))))
+    return;
+  state[si] = buf[bi];
+}
+
+static int halo_copy(lbm_solver *s, int xplane, int sgn, void *buf, int to_buf,
+    int guarded = 0)
+{
+  dim3 block(32, 8, 1);
+  dim3 grid((s->ub.nz + 31) / 32, (s->ub.ny + 7) / 8, 5);
+  void *st = s->pattern == LBM_AA ? s->buf[0] : s->buf[s->cur];
+  switch (storage_size(s->precision)) {
+  case 8:
+    halo_copy_kernel<uint64_t><<<grid, block, 0, s->stream>>>(s->g, s->ub, xplane, sgn,
+        (uint64_t *)st, (uint64_t *)buf, to_buf, s->mask, guarded);
+    break;
+  case 4:
+    halo_copy_kernel<uint32_t><<<grid, block, 0, s->stream>>>(s->g, s->ub, xplane, sgn,
+        (uint32_t *)st, (uint32_t *)buf, to_buf, s->mask, guarded);
+    break;
+  default:
+    halo_copy_kernel<uint16_t><<<grid, block, 0, s->stream>>>(s->g, s->ub, xplane, sgn,
+        (uint16_t *)st, (uint16_t *)buf, to_buf, s->mask, guarded);
+  }
+  CUDA_TRY(cudaGetLastError());
+  return LBM_OK;
+}
+
+extern "C" size_t lbm_halo_bytes(const lbm_solver *s)
+{
+  if (!s || !s->slab)
+    return 0;
+  return (size_t)5 * s->ub.ny * s->ub.nz * storage_size(s->precision);
+}
+
+extern "C" int lbm_halo_shifted(const lbm_solver *s)
+{
+  return s && s->slab && orientation(s) != kNatural;
+}
+
+extern "C" int lbm_halo_needs(const lbm_solver *s)
+{
+  if (!s || !s->slab)
+    return 0;
+  if (s->pattern == LBM_PULL)
+    return LBM_HALO_BEFORE;
+  if (s->pattern == LBM_PUSH)
+    return LBM_HALO_AFTER;
+  return (s->steps_done & 1) ? (LBM_HALO_BEFORE | LBM_HALO_AFTER) : 0;
+}
+
+static int halo_check(const lbm_solver *s, int when, const void *a, const void *b,
+    const char *fn)
+{
+  if (!s || !s->slab || !a || !b)
+    return fail(LBM_ERR_ARG, "%s: needs a slab solver and two device buffers", fn);
+  if (when != LBM_HALO_BEFORE && when != LBM_HALO_AFTER && when != LBM_HALO_SCATTER)
+    return fail(LBM_ERR_ARG, "%s: when = %d is not LBM_HALO_BEFORE, _AFTER or _SCATTER", fn,
+        when);
+  // before: the next step's needs (and a shifted state's ghost data, which
+  // are the same slots); after: the last step's; scatter: shifted states
+  bool ok;
+  if (when == LBM_HALO_SCATTER)
+    ok = lbm_halo_shifted(s);
+  else if (s->pattern == LBM_PULL)
+    ok = when == LBM_HALO_BEFORE;
+  else if (s->pattern == LBM_PUSH)
+    ok = when == LBM_HALO_AFTER;
+  else
+    ok = when == LBM_HALO_BEFORE ? (s->steps_done & 1) : (s->steps_done > 0 && !(s->steps_done & 1));
+  if (!ok)
+    return fail(LBM_ERR_STATE, "%s: no %s exchange at step %lld of this pattern", fn,
+        when == LBM_HALO_BEFORE ? "before-step" : when == LBM_HALO_AFTER ? "after-step" :
+        "scatter", s->steps_done);
+  CUDA_TRY(cudaSetDevice(s->device));
+  return LBM_OK;
+}
+
+extern "C" int lbm_halo_pack(lbm_solver *s, int when, void *to_left, void *to_right)
+{
+  int rc = halo_check(s, when, to_left, to_right, "lbm_halo_pack");
+  if (rc)
+    return rc;
+  const int first = 1, last = s->g.nx - 2;
+  // slots of a shifted state in the left ghost: pull P, AA M (right: opposite)
+  const int left_ghost_set = s->pattern == LBM_PULL ? +1 : -1;
+  if (when == LBM_HALO_BEFORE) {
+    if ((rc = halo_copy(s, last, left_ghost_set, to_right, 1)))
+      return rc;
+    return halo_copy(s, first, -left_ghost_set, to_left, 1);
+  }
+  if (when == LBM_HALO_SCATTER) {
+    if ((rc = halo_copy(s, 0, left_ghost_set, to_left, 1)))
+      return rc;
+    return halo_copy(s, s->g.nx - 1, -left_ghost_set, to_right, 1);
+  }
+  if ((rc = halo_copy(s, s->g.nx - 1, +1, to_right, 1)))
+    return rc;
+  return halo_copy(s, 0, -1, to_left, 1);
+}
+
+extern "C" int lbm_halo_unpack(lbm_solver *s, int when, const void *from_left,
+    const void *from_right)
+{
+  int rc = halo_check(s, when, from_left, from_right, "lbm_halo_unpack");
+  if (rc)
+    return rc;
+  const int first = 1, last = s->g.nx - 2;
+  const int left_ghost_set = s->pattern == LBM_PULL ? +1 : -1;
+  if (when == LBM_HALO_BEFORE) {
+    // the left slab sent its last plane's slots of our left ghost's set
+    if ((rc = halo_copy(s, 0, left_ghost_set, (void *)from_left, 0)))
+      return rc;
+    return halo_copy(s, s->g.nx - 1, -left_ghost_set, (void *)from_right, 0);
+  }
+  if (when == LBM_HALO_SCATTER) {
+    // the left slab sent its right ghost (our first plane's share of its
+    // boundary cells' populations); the pull state keeps population d of
+    // x + c_d in slot d of x, the AA state population inv d of x - c_d
+    const int gm = s->pattern == LBM_PULL ? kGuardOwn : kGuardInv;
+    if ((rc = halo_copy(s, first, -left_ghost_set, (void *)from_left, 0, gm)))
+      return rc;
+    return halo_copy(s, last, left_ghost_set, (void *)from_right, 0, gm);
+  }
+  if ((rc = halo_copy(s, first, +1, (void *)from_left, 0, kGuardInv)))
+    return rc;
+  return halo_copy(s, last, -1, (void *)from_right, 0, kGuardInv);
+}
+
+extern "C" void *lbm_stream(const lbm_solver *s) { return s ? (void *)s->stream : NULL; }
+
+// ---------------------------------------------------------------------------
+// Seeded initial state on the device
+// ---------------------------------------------------------------------------
+
+// splitmix64 (Steele, Lea, Flood 2014), the same counter-based stream as
+// lbm_perturbed_equilibrium in host/lbm_host.c: cell c (caller's dense
+// index) draws from state seed ^ mix(c * golden + 1), advanced by the
+// golden-ratio increment, so host and device produce identical values.
+__device__ __forceinline__ uint64_t mix64_d(uint64_t z)
+{
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+template <class ST>
+__global__ void init_equilibrium_kernel(Grid g, UserBox u, int orient, typename ST::S *state,
+    const uint32_t *__restrict__ mask, unsigned long long seed, double amp, double rho, float scale)
+{
+  using V = typename ST::V;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= u.nz || y >= u.ny)
+    return;
+  const uint32_t cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
+  const uint32_t m = mask[cell];
+  if (m & kSolidBit)
+    return;
+  const long long c = dense_index(u, x, y, z);
+  uint64_t st = (uint64_t)seed ^ mix64_d((uint64_t)c * 0x9E3779B97F4A7C15ull + 1ull);
+  // explicit round-to-nearest operations: no multiply-add contraction, so
+  // the values equal the host generator's (compiled without contraction)
+  double uu[3];
+  for (int k = 0; k < 3; ++k) {
+    st += 0x9E3779B97F4A7C15ull;
+    const double r = __dmul_rn((double)(mix64_d(st) >> 11), 1.0 / 9007199254740992.0);
+    uu[k] = __dmul_rn(amp, __dadd_rn(__dmul_rn(2.0, r), -1.0));
+  }
+  const double usq = __dadd_rn(__dadd_rn(__dmul_rn(uu[0], uu[0]), __dmul_rn(uu[1], uu[1])),
+      __dmul_rn(uu[2], uu[2]));
+  const Offs nb = make_offs(g, x + u.ox, y + u.oy, z + u.oz);
+#pragma unroll
+  for (int d = 0; d < Q; ++d) {
+    const int wc = wclass(d);
+    const double w = wc == 0 ? 1.0 / 3.0 : wc == 1 ? 1.0 / 18.0 : 1.0 / 36.0;
+    const double cu = __dadd_rn(__dadd_rn(__dmul_rn(cx(d), uu[0]), __dmul_rn(cy(d), uu[1])),
+        __dmul_rn(cz(d), uu[2]));
+    const double t = __dadd_rn(__dadd_rn(__dadd_rn(rho, -__dmul_rn(1.5, usq)),
+        __dmul_rn(3.0, cu)), __dmul_rn(__dmul_rn(4.5, cu), cu));
+    double v = __dmul_rn(w, t);
+    if (ST::kShifted)
+      v = __dadd_rn(v, -w);
+    int p;
+    uint32_t sc;
+    state_slot(orient, d, m, cell, nb, p, sc);
+    ST::store(state + (long long)p * g.plane + sc, (V)v, (V)scale);
+  }
+}
+
+template <class ST> static int init_eq_t(lbm_solver *s, unsigned long long seed, double amp,
+    double rho)
+{
+  dim3 grid, block;
+  user_launch_shape(s, grid, block);
+  init_equilibrium_kernel<ST><<<grid, block, 0, s->stream>>>(s->g, s->ub, orientation(s),
+      (typename ST::S *)state_ptr(s), s->mask, seed, amp, rho,
+      (float)(s->precision == LBM_F16 ? s->fp16_scale : 1.0));
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return LBM_OK;
+}
+
+extern "C" int lbm_init_equilibrium(lbm_solver *s, unsigned long long seed, double amplitude,
+    double rho)
+{
+  if (!s)
+    return fail(LBM_ERR_ARG, "lbm_init_equilibrium: NULL solver");
+  CUDA_TRY(cudaSetDevice(s->device));
+  switch (s->precision) {
+  case LBM_F64: return init_eq_t<StoreF64>(s, seed, amplitude, rho);
+  case LBM_F32: return init_eq_t<StoreF32>(s, seed, amplitude, rho);
+  default: return init_eq_t<StoreF16>(s, seed, amplitude, rho);
+  }
+}
+
+extern "C" int lbm_device_memory(size_t *free_bytes, size_t *total_bytes)
+{
+  size_t f = 0, t = 0;
+  CUDA_TRY(cudaMemGetInfo(&f, &t));
+  if (free_bytes)
+    *free_bytes = f;
+  if (total_bytes)
+    *total_bytes = t;
+  return LBM_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Adjoint of the Brinkman step with checkpointing
 // ---------------------------------------------------------------------------
 
@@ -1283,6 +1599,8 @@ extern "C" int lbm_adjoint_gradient(lbm_solver *s, int steps, int checkpoint_eve
     return fail(LBM_ERR_ARG, "lbm_adjoint_gradient: bad arguments");
   if (s->pattern != LBM_AA)
     return fail(LBM_ERR_ARG, "lbm_adjoint_gradient: needs an AA solver");
+  if (s->slab)
+    return fail(LBM_ERR_ARG, "lbm_adjoint_gradient: not available on slab solvers");
   if (s->precision == LBM_F16)
     return fail(LBM_ERR_ARG, "lbm_adjoint_gradient: FP16 storage is not supported (FP64/FP32)");
   if (!s->porosity || s->alpha == 0.0)
@@ -1293,13 +1611,36 @@ extern "C" int lbm_adjoint_gradient(lbm_solver *s, int steps, int checkpoint_eve
   const size_t P = (size_t)s->g.plane;
   const size_t ubytes = 3 * P * vs;  // momentum of one step
   const size_t lbytes = Q * P * vs;  // one adjoint lattice
-  // checkpoint interval: given, or the one that minimises checkpoints
-  // (steps/k states) plus the segment's saved momenta (k momentum sets)
+  // checkpoint interval: given; 0 = the one that minimises checkpoints
+  // (steps/k states) plus the segment's saved momenta (k momentum sets);
+  // LBM_CKPT_AUTO = the longest interval (least recomputation: steps - k
+  // steps are recomputed) whose memory fits in 90% of the free device memory
+  const auto mem_for = [&](long long kk) {
+    return (double)((steps + kk - 1) / kk) * (double)s->state_bytes + (double)kk * ubytes +
+        2.0 * lbytes + (double)P * 8;
+  };
   int k = checkpoint_every;
-  if (k <= 0) {
-    k = (int)ceil(sqrt((double)steps * (double)s->state_bytes / (double)ubytes));
-    if (k < 1)
-      k = 1;
+  const int k_sqrt = std::max(1, (int)ceil(sqrt((double)steps * (double)s->state_bytes /
+      (double)ubytes)));
+  if (k == LBM_CKPT_AUTO) {
+    size_t free_b = 0, total_b = 0;
+    CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    const double budget = 0.9 * (double)free_b;
+    k = std::min(k_sqrt, steps);
+    // memory grows with k beyond k_sqrt; the largest fitting k by bisection
+    long long lo = k, hi = steps;
+    if (mem_for(hi) <= budget)
+      lo = hi;
+    while (hi - lo > 1) {
+      const long long mid = (lo + hi) / 2;
+      if (mem_for(mid) <= budget)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    k = (int)lo;
+  } else if (k <= 0) {
+    k = k_sqrt;
   }
   if (k > steps)
     k = steps;
@@ -1322,12 +1663,24 @@ extern "C" int lbm_adjoint_gradient(lbm_solver *s, int steps, int checkpoint_eve
     const long long t0 = s->steps_done;
     void *state = s->buf[0];
 
-    // forward sweep: checkpoint every k steps
+    // forward sweep: checkpoint every k steps; the last segment saves its
+    // momenta directly, so the reverse sweep does not recompute it
     ATRY(cudaEventRecord(e0, s->stream));
     for (int c = 0; c < nck; ++c) {
       ATRY(cudaMemcpyAsync(ck + (size_t)c * s->state_bytes, state, s->state_bytes,
           cudaMemcpyDeviceToDevice, s->stream));
-      RTRY(lbm_run(s, std::min(k, steps - c * k)));
+      const int len = std::min(k, steps - c * k);
+      if (c < nck - 1) {
+        RTRY(lbm_run(s, len));
+        continue;
+      }
+      for (int i = 0; i < len; ++i) {
+        s->u_save_next = ub + (size_t)i * ubytes;
+        rc = launch_one(s, NULL);
+        s->u_save_next = NULL;
+        if (rc)
+          goto done;
+      }
     }
     ATRY(cudaEventRecord(e1, s->stream));
     ATRY(cudaEventSynchronize(e1));
@@ -1348,10 +1701,12 @@ extern "C" int lbm_adjoint_gradient(lbm_solver *s, int steps, int checkpoint_eve
     float adj_ms = 0.f;
     for (int c = nck - 1; c >= 0; --c) {
       const int tc = c * k, len = std::min(k, steps - tc);
-      ATRY(cudaMemcpyAsync(state, ck + (size_t)c * s->state_bytes, s->state_bytes,
-          cudaMemcpyDeviceToDevice, s->stream));
-      s->steps_done = t0 + tc;
-      for (int i = 0; i < len; ++i) {
+      if (c < nck - 1) {
+        ATRY(cudaMemcpyAsync(state, ck + (size_t)c * s->state_bytes, s->state_bytes,
+            cudaMemcpyDeviceToDevice, s->stream));
+        s->steps_done = t0 + tc;
+      }
+      for (int i = 0; i < len && c < nck - 1; ++i) {
         s->u_save_next = ub + (size_t)i * ubytes;
         rc = launch_one(s, NULL);
         s->u_save_next = NULL;

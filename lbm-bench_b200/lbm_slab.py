@@ -1,0 +1,202 @@
+"""x-slab decomposition of one lattice over a ring of slabs.
+
+The domain is cut along x - the slowest axis of LBM-Bench's SoA index
+(src/lbm.h:113-116) and the periodic axis of its channel geometries - into
+one slab per rank (one GPU each). A slab is a solver made by lbm_create_slab:
+its own planes plus one ghost plane per side holding the neighbour's
+boundary cells. Per step only the five populations that cross an x face move
+between ring neighbours (lbm_halo_* in include/lbm_b200.h): one message pair
+before a pull or AA odd step, one after a push or AA odd step, none around an
+AA even step. Results are bit-identical to the undecomposed solver.
+
+The pull state, and the AA state after an odd number of steps, keep part of
+a boundary cell's populations in the neighbour's cells: call scatter() after
+setting slab states and gather() before reading them.
+
+Transport: torch.distributed point-to-point (NCCL over NVLink between GPUs,
+gloo between CPU processes), ordered on the solver's CUDA stream, so the
+exchange never blocks the host. `LocalRing` runs several slabs of one
+process (on one or several devices) with device copies instead.
+
+LBM-Bench itself has no decomposition (single-node OpenMP, src/main.c).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+import lbmb200 as L
+
+
+# ---------------------------------------------------------------------------
+# partition
+# ---------------------------------------------------------------------------
+
+def split(nx: int, world: int, rank: int):
+    """Planes [x0, x1) of slab `rank`: the first nx % world slabs get one
+    plane more."""
+    if world < 1 or not 0 <= rank < world or nx < world:
+        raise ValueError(f"cannot split {nx} planes over {world} slabs (rank {rank})")
+    q, r = divmod(nx, world)
+    x0 = rank * q + min(rank, r)
+    return x0, x0 + q + (1 if rank < r else 0)
+
+
+def slab_flags(flags: np.ndarray, x0: int, x1: int) -> np.ndarray:
+    """Flags (nz, ny, nx) of the whole x-periodic domain -> the slab's flags
+    with the neighbours' boundary planes (x0 - 1 and x1, wrapped) around it."""
+    nx = flags.shape[2]
+    idx = [(x0 - 1) % nx] + list(range(x0, x1)) + [x1 % nx]
+    return np.ascontiguousarray(flags[:, :, idx])
+
+
+# ---------------------------------------------------------------------------
+# transports
+# ---------------------------------------------------------------------------
+
+class Ring:
+    """Point-to-point exchange with the two ring neighbours over a
+    torch.distributed process group (all ranks call exchange() together).
+
+    Messages are tagged by direction (1: travelling right, 2: travelling
+    left), and every rank posts its operations in the same order - send
+    right, send left, receive from left, receive from right - so that with
+    two ranks, where both neighbours are the same peer, the i-th send to a
+    peer meets that peer's i-th receive from it."""
+
+    def __init__(self, group=None):
+        import torch.distributed as dist
+        self.dist = dist
+        self.group = group
+        if dist.is_available() and dist.is_initialized():
+            self.rank = dist.get_rank(group)
+            self.world = dist.get_world_size(group)
+        else:
+            self.rank, self.world = 0, 1
+        self.left = (self.rank - 1) % self.world
+        self.right = (self.rank + 1) % self.world
+        if group is not None and self.world > 1:
+            self.left = dist.get_global_rank(group, self.left)
+            self.right = dist.get_global_rank(group, self.right)
+
+    def exchange(self, send_left, send_right, recv_left, recv_right):
+        if self.world == 1:  # both neighbours are this slab: periodic in x
+            recv_left.copy_(send_right)
+            recv_right.copy_(send_left)
+            return
+        d = self.dist
+        ops = [d.P2POp(d.isend, send_right, self.right, self.group, tag=1),
+               d.P2POp(d.isend, send_left, self.left, self.group, tag=2),
+               d.P2POp(d.irecv, recv_left, self.left, self.group, tag=1),
+               d.P2POp(d.irecv, recv_right, self.right, self.group, tag=2)]
+        for w in d.batch_isend_irecv(ops):
+            w.wait()
+
+
+class SlabRunner:
+    """Steps one slab of a ring: exchange, step, exchange, as the pattern
+    and the step parity need (Solver.halo_needs).
+
+    `solver` is a slab (Solver.slab) or any object with the same halo_*
+    methods, run() and stream; `device` is where the message buffers live
+    ("cuda" for a GPU slab)."""
+
+    def __init__(self, solver, ring: Ring, device="cuda"):
+        import torch
+        self.torch = torch
+        self.s = solver
+        self.ring = ring
+        n = solver.halo_bytes
+        if n <= 0:
+            raise ValueError("SlabRunner needs a slab solver (lbm_create_slab)")
+        self.bufs = [torch.empty(n, dtype=torch.uint8, device=device) for _ in range(4)]
+        self.ext = None
+        dev = torch.device(device)
+        if dev.type == "cuda":
+            if dev.index is None:
+                dev = torch.device("cuda", torch.cuda.current_device())
+            self.ext = torch.cuda.ExternalStream(solver.stream, device=dev)
+        self.exchanges = 0
+
+    def _exchange(self, when: int):
+        sl, sr, rl, rr = self.bufs
+        self.s.halo_pack(when, sl, sr)
+        if self.ext is not None:
+            with self.torch.cuda.stream(self.ext):
+                self.ring.exchange(sl, sr, rl, rr)
+        else:
+            self.ring.exchange(sl, sr, rl, rr)
+        self.s.halo_unpack(when, rl, rr)
+        self.exchanges += 1
+
+    def run(self, steps: int):
+        for _ in range(steps):
+            need = self.s.halo_needs
+            if need & L.HALO_BEFORE:
+                self._exchange(L.HALO_BEFORE)
+            self.s.run(1)
+            if need & L.HALO_AFTER:
+                self._exchange(L.HALO_AFTER)
+
+    def gather(self):
+        """Before reading the state: the neighbours' share of this slab's
+        boundary populations into the ghost planes (shifted states only)."""
+        if self.s.halo_shifted:
+            self._exchange(L.HALO_BEFORE)
+
+    def scatter(self):
+        """After setting the state: the boundary populations set_state kept
+        in the ghost planes go to the neighbours (shifted states only)."""
+        if self.s.halo_shifted:
+            self._exchange(L.HALO_SCATTER)
+
+
+class LocalRing:
+    """Several slabs of one ring driven from one process: every slab packs,
+    all streams are synchronised, every slab unpacks its neighbours'
+    messages. For tests and for domains split over the devices of one
+    process; the kernels of different slabs never wait on one another."""
+
+    def __init__(self, solvers, device="cuda"):
+        import torch
+        self.solvers = list(solvers)
+        self.bufs = []
+        for s in self.solvers:
+            n = s.halo_bytes
+            if n <= 0:
+                raise ValueError("LocalRing needs slab solvers (lbm_create_slab)")
+            self.bufs.append([torch.empty(n, dtype=torch.uint8, device=device) for _ in range(2)])
+
+    def _exchange(self, when: int):
+        n = len(self.solvers)
+        for s, (tl, tr) in zip(self.solvers, self.bufs):
+            s.halo_pack(when, tl, tr)
+        for s in self.solvers:
+            s.synchronize()
+        for i, s in enumerate(self.solvers):
+            left, right = self.bufs[(i - 1) % n], self.bufs[(i + 1) % n]
+            s.halo_unpack(when, left[1], right[0])  # left's to_right, right's to_left
+        for s in self.solvers:
+            s.synchronize()
+
+    def run(self, steps: int):
+        for _ in range(steps):
+            needs = {s.halo_needs for s in self.solvers}
+            if len(needs) != 1:
+                raise RuntimeError("slabs of one ring are at different steps")
+            need = needs.pop()
+            if need & L.HALO_BEFORE:
+                self._exchange(L.HALO_BEFORE)
+            for s in self.solvers:
+                s.run(1)
+            if need & L.HALO_AFTER:
+                self._exchange(L.HALO_AFTER)
+
+    def gather(self):
+        """Before reading the slabs' states (see SlabRunner.gather)."""
+        if self.solvers[0].halo_shifted:
+            self._exchange(L.HALO_BEFORE)
+
+    def scatter(self):
+        """After setting the slabs' states (see SlabRunner.scatter)."""
+        if self.solvers[0].halo_shifted:
+            self._exchange(L.HALO_SCATTER)

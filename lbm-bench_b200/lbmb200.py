@@ -21,6 +21,8 @@ LIB_PATH = os.environ.get("LBMB200_LIB") or os.path.join(HERE, "liblbmb200.so")
 
 PUSH, PULL, AA = 0, 1, 2
 F64, F32, F16 = 0, 1, 2
+CKPT_AUTO = -1  # lbm_adjoint_gradient: least recomputation that fits in device memory
+HALO_BEFORE, HALO_AFTER, HALO_SCATTER = 1, 2, 4
 PATTERNS = {"push": PUSH, "pull": PULL, "aa": AA}
 PRECISIONS = {"fp64": F64, "fp32": F32, "fp16": F16}
 Q = 19
@@ -45,6 +47,15 @@ _SIGNATURES = [
     ("lbm_create", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                   _ip, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_int]),
+    ("lbm_create_slab", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int]),
+    ("lbm_halo_bytes", ctypes.c_size_t, [_vp]),
+    ("lbm_halo_needs", ctypes.c_int, [_vp]),
+    ("lbm_halo_shifted", ctypes.c_int, [_vp]),
+    ("lbm_halo_pack", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
+    ("lbm_halo_unpack", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
+    ("lbm_stream", _vp, [_vp]),
     ("lbm_destroy", ctypes.c_int, [_vp]),
     ("lbm_set_params", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                       ctypes.c_int]),
@@ -64,6 +75,10 @@ _SIGNATURES = [
     ("lbm_mass_momentum_noalloc", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int,
                                                  ctypes.c_int, _dp, _llp, _vp]),
     ("lbm_objective", ctypes.c_int, [_vp, _dp]),
+    ("lbm_init_equilibrium", ctypes.c_int, [_vp, ctypes.c_ulonglong, ctypes.c_double,
+                                            ctypes.c_double]),
+    ("lbm_device_memory", ctypes.c_int, [ctypes.POINTER(ctypes.c_size_t),
+                                         ctypes.POINTER(ctypes.c_size_t)]),
     ("lbm_adjoint_gradient", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp]),
     ("lbm_set_state_padded", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int]),
     ("lbm_get_state_padded", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int]),
@@ -115,6 +130,17 @@ def device_count() -> int:
     return lib().lbm_device_count()
 
 
+def device_memory():
+    """(free, total) bytes of the current CUDA device."""
+    f, t = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    _check(lib().lbm_device_memory(ctypes.byref(f), ctypes.byref(t)))
+    return f.value, t.value
+
+
+def _addr(buf) -> int:
+    return buf if isinstance(buf, int) else buf.data_ptr()
+
+
 class Solver:
     """One device lattice (include/lbm_b200.h lbm_create ... lbm_destroy)."""
 
@@ -133,6 +159,58 @@ class Solver:
         _check(lib().lbm_create(ctypes.byref(h), nx, ny, nz, _p(flags, _ip), *self.periodic,
                                 pattern, precision))
         self._h = h
+
+    @classmethod
+    def slab(cls, flags, periodic_yz=(0, 0), pattern=AA, precision=F64):
+        """x-slab of a decomposed domain (lbm_create_slab): `flags` has the
+        slab's planes plus the neighbours' boundary planes at x = 0 and
+        x = -1 (shape (nz, ny, nx + 2))."""
+        self = cls.__new__(cls)
+        if isinstance(pattern, str):
+            pattern = PATTERNS[pattern]
+        if isinstance(precision, str):
+            precision = PRECISIONS[precision]
+        flags = np.ascontiguousarray(flags, dtype=np.int32)
+        nz, ny, nxg = flags.shape
+        nx = nxg - 2
+        self.shape = (nx, ny, nz)
+        self.flags = flags
+        self.pattern, self.precision = pattern, precision
+        self.periodic = (0,) + tuple(int(p) for p in periodic_yz)
+        h = _vp()
+        _check(lib().lbm_create_slab(ctypes.byref(h), nx, ny, nz, _p(flags, _ip),
+                                     *self.periodic[1:], pattern, precision))
+        self._h = h
+        return self
+
+    # -- halo exchange (slab solvers) --------------------------------------
+    @property
+    def halo_bytes(self) -> int:
+        return lib().lbm_halo_bytes(self._h)
+
+    @property
+    def halo_needs(self) -> int:
+        """Exchanges the next step takes: HALO_BEFORE | HALO_AFTER bits."""
+        return lib().lbm_halo_needs(self._h)
+
+    @property
+    def halo_shifted(self) -> bool:
+        """The state keeps boundary populations in the ghost planes: exchange
+        HALO_BEFORE before reading it, HALO_SCATTER after setting it."""
+        return bool(lib().lbm_halo_shifted(self._h))
+
+    def halo_pack(self, when: int, to_left, to_right) -> None:
+        """Writes the messages for the left and right neighbours into device
+        buffers (integer addresses or objects with data_ptr())."""
+        _check(lib().lbm_halo_pack(self._h, when, _addr(to_left), _addr(to_right)))
+
+    def halo_unpack(self, when: int, from_left, from_right) -> None:
+        _check(lib().lbm_halo_unpack(self._h, when, _addr(from_left), _addr(from_right)))
+
+    @property
+    def stream(self) -> int:
+        """The solver's cudaStream_t as an integer."""
+        return lib().lbm_stream(self._h) or 0
 
     # -- lifecycle ---------------------------------------------------------
     def close(self) -> None:
@@ -169,6 +247,10 @@ class Solver:
         if f.shape != (Q,) + self.shape:
             raise ValueError(f"state shape {f.shape} != {(Q,) + self.shape}")
         _check(lib().lbm_set_state(self._h, _p(f, _dp)))
+
+    def init_equilibrium(self, seed=1, amplitude=1e-4, rho=1.0):
+        """Device-side lbm_perturbed_equilibrium (lbm_init_equilibrium)."""
+        _check(lib().lbm_init_equilibrium(self._h, seed, amplitude, rho))
 
     def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
         if out is None:
@@ -230,7 +312,9 @@ class Solver:
 
     def adjoint_gradient(self, steps: int, checkpoint_every: int = 0):
         """dJ/dphi after `steps` Brinkman steps from the current state
-        (lbm_adjoint_gradient). Returns (J, grad[nx, ny, nz], info dict)."""
+        (lbm_adjoint_gradient). checkpoint_every: interval, 0 for the sqrt
+        schedule, CKPT_AUTO for the least recomputation that fits in device
+        memory. Returns (J, grad[nx, ny, nz], info dict)."""
         grad = np.zeros(self.shape)
         j = ctypes.c_double(0.0)
         info = np.zeros(6)

@@ -57,10 +57,15 @@ def test_adjoint_matches_oracle(oracle):
 def test_gradient_independent_of_checkpoint_interval():
     flags, per, por, f0 = _case((16, 12, 12), 5)
     grads = []
-    for k in (1, 6, 25, 0):
+    infos = []
+    for k in (1, 6, 25, 0, L.CKPT_AUTO):
         with _solver(flags, per, por, f0) as s:
-            _, g, _ = s.adjoint_gradient(25, checkpoint_every=k)
+            _, g, info = s.adjoint_gradient(25, checkpoint_every=k)
             grads.append(g)
+            infos.append(info)
+    # the memory-aware schedule has room for every step's momentum here:
+    # one segment, saved by the forward sweep, nothing recomputed
+    assert infos[-1]["interval"] == 25 and infos[-1]["checkpoints"] == 1
     for g in grads[1:]:
         assert np.array_equal(g, grads[0])
 

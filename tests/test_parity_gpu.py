@@ -201,3 +201,15 @@ def test_full_size_conservation_in_periodic_box(pattern):
     assert abs(t1[0] - t0[0]) <= 1e-12 * t0[0]
     assert t1[1] - t0[1] == pytest.approx(F * cells * steps, rel=1e-9)
     assert abs(t1[2] - t0[2]) < 1e-9 and abs(t1[3] - t0[3]) < 1e-9
+
+
+@pytest.mark.parametrize("pattern", PATTERNS)
+@pytest.mark.parametrize("precision", [L.F64, L.F16])
+def test_device_initial_state_equals_host_generator(pattern, precision):
+    flags, frac, _ = L.porous_channel((20, 18, 16), 0.2, 2.0, 3.0, seed=4)
+    f0 = L.perturbed_equilibrium(flags, seed=77, amplitude=1e-3)
+    with L.Solver(flags, (1, 0, 0), pattern, precision) as a, \
+            L.Solver(flags, (1, 0, 0), pattern, precision) as b:
+        a.set_state(f0)
+        b.init_equilibrium(seed=77, amplitude=1e-3)
+        assert np.array_equal(a.get_state(), b.get_state())
