@@ -6,6 +6,7 @@
 
 #include "lbm_adjoint.cuh"
 #include "lbm_step.cuh"
+#include "lbm_step_tma.cuh"
 #include "lbm_step_x2.cuh"
 
 namespace lbm {
@@ -17,6 +18,10 @@ enum Precision { kF64 = 0, kF32 = 1, kF16 = 2 };
 // cells per thread (lbm_step_lp.cu).
 cudaError_t launch_step_f64(int kind, bool force, bool brink, const StepArgs<StoreF64> &a,
     dim3 grid, dim3 block, cudaStream_t st);
+// Bulk-copy pipelined FP64 step (lbm_step_tma.cuh): `groups` consumer
+// groups of 8 warps (1..3), `blocks` persistent CTAs.
+cudaError_t launch_step_tma_f64(int kind, bool force, const TmaArgs<StoreF64> &a, int groups,
+    int blocks, cudaStream_t st);
 cudaError_t launch_step_x2_f32(int kind, bool force, bool brink, const StepArgs2<StoreF32> &a,
     cudaStream_t st);
 cudaError_t launch_step_x2_f16(int kind, bool force, bool brink, const StepArgs2<StoreF16> &a,

@@ -73,6 +73,10 @@ struct lbm_solver {
   int no_shuffle; // reduced precision: never use the shuffle-aligned kernels
   void *u_save_next; // adjoint recomputation: momentum output of the next step
   int slab;          // x-slab of a decomposed domain: device planes 0 and nx+1 are ghosts
+  int tma;           // FP64 steps use the bulk-copy pipelined kernels (shape in tma_shape)
+  int tma_groups;    // consumer groups of 8 warps per CTA
+  TmaShape tma_shape;
+  unsigned int *dev_err; // set by kernels whose bounded waits ran out
 };
 
 extern "C" const char *lbm_last_error(void) { return g_err; }
@@ -485,6 +489,7 @@ static void free_all(lbm_solver *s)
   cudaFree(s->staging);
   cudaFree(s->pstaging);
   cudaFree(s->red);
+  cudaFree(s->dev_err);
   if (s->ev[0])
     cudaEventDestroy(s->ev[0]);
   if (s->ev[1])
@@ -629,6 +634,34 @@ static int create_impl(lbm_solver **out, int nx, int ny, int nz, const int *flag
   TRYC(cudaMemsetAsync(s->buf[0], 0, s->state_bytes, s->stream));
   if (s->buf[1])
     TRYC(cudaMemsetAsync(s->buf[1], 0, s->state_bytes, s->stream));
+
+  TRY(dev_alloc(s, (void **)&s->dev_err, sizeof(unsigned int), "the kernel error word"));
+  TRYC(cudaMemsetAsync(s->dev_err, 0, sizeof(unsigned int), s->stream));
+  {
+    // pipelined FP64 kernels (lbm_step_tma.cuh): with LBM_B200_TMA=1;
+    // LBM_B200_TMA_T / _STAGES / _GROUPS set the tile rows, pipeline depth
+    // and consumer groups
+    const char *e = getenv("LBM_B200_TMA");
+    const auto env_int = [](const char *n) {
+      const char *v = getenv(n);
+      return v ? atoi(v) : 0;
+    };
+    int optin = 0, sms = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+    s->tma = precision == LBM_F64 && e && e[0] == '1' && optin > 1024 &&
+        tma_shape(s->g, storage_size(precision), env_int("LBM_B200_TMA_T"),
+            env_int("LBM_B200_TMA_STAGES"), (size_t)optin - 1024, s->tma_shape);
+    s->tma_groups = env_int("LBM_B200_TMA_GROUPS");
+    if (s->tma_groups < 1 || s->tma_groups > 3)
+      s->tma_groups = 2;
+    if (s->tma) {
+      // each stage belongs to one consumer group: a multiple of the groups
+      s->tma_shape.stages -= s->tma_shape.stages % s->tma_groups;
+      s->tma = s->tma_shape.stages >= s->tma_groups;
+      s->tma_shape.blocks = s->tma_shape.ntiles < sms ? s->tma_shape.ntiles : sms;
+    }
+  }
 
   // fluid bytes in device cell order (frames and padding = wall), then the masks
   std::vector<uint8_t> fluid((size_t)cells, 0);
@@ -1001,7 +1034,19 @@ static int launch_one(lbm_solver *s, int *kind_out)
     a.porosity = s->porosity;
     a.u_save = brink ? (double *)s->u_save_next : nullptr;
     a.c = make_consts<double>(s);
-    e = launch_step_f64(kind, force, brink, a, grid, block, s->stream);
+    if (s->tma && !brink) {
+      TmaArgs<StoreF64> t;
+      t.s = a;
+      t.T = s->tma_shape.T;
+      t.stages = s->tma_shape.stages;
+      t.ytiles = s->tma_shape.ytiles;
+      t.ntiles = s->tma_shape.ntiles;
+      t.stage_bytes = s->tma_shape.stage_bytes;
+      t.err = s->dev_err;
+      e = launch_step_tma_f64(kind, force, t, s->tma_groups, s->tma_shape.blocks, s->stream);
+    } else {
+      e = launch_step_f64(kind, force, brink, a, grid, block, s->stream);
+    }
   } else if (s->precision == LBM_F32) {
     StepArgs2<StoreF32> a;
     a.g = s->g;
@@ -1049,12 +1094,25 @@ extern "C" int lbm_run(lbm_solver *s, int steps)
   return LBM_OK;
 }
 
+// Reads the kernels' error word after the stream has drained.
+static int check_kernel_error(lbm_solver *s)
+{
+  unsigned int err = 0;
+  CUDA_TRY(cudaMemcpy(&err, s->dev_err, sizeof(err), cudaMemcpyDeviceToHost));
+  if (err) {
+    CUDA_TRY(cudaMemset(s->dev_err, 0, sizeof(err)));
+    return fail(LBM_ERR_CUDA, "a pipelined step kernel gave up waiting for its bulk copies; "
+        "the state is undefined");
+  }
+  return LBM_OK;
+}
+
 extern "C" int lbm_synchronize(lbm_solver *s)
 {
   if (!s)
     return fail(LBM_ERR_ARG, "lbm_synchronize: NULL solver");
   CUDA_TRY(cudaStreamSynchronize(s->stream));
-  return LBM_OK;
+  return check_kernel_error(s);
 }
 
 extern "C" int lbm_run_timed(lbm_solver *s, int steps, double *ms)
@@ -1072,7 +1130,7 @@ extern "C" int lbm_run_timed(lbm_solver *s, int steps, double *ms)
   float t = 0.f;
   CUDA_TRY(cudaEventElapsedTime(&t, s->ev[0], s->ev[1]));
   *ms = t;
-  return LBM_OK;
+  return check_kernel_error(s);
 }
 
 extern "C" int lbm_time_launches(lbm_solver *s, int steps, double *ms_sum, int *count,
@@ -1114,7 +1172,7 @@ extern "C" int lbm_time_launches(lbm_solver *s, int steps, double *ms_sum, int *
     return rc;
   if (e != cudaSuccess)
     return fail(LBM_ERR_CUDA, "lbm_time_launches: %s", cudaGetErrorString(e));
-  return LBM_OK;
+  return check_kernel_error(s);
 }
 
 template <class ST> static int moments_t(lbm_solver *s, double *q[4])
