@@ -15,8 +15,9 @@ time, state resident in HBM, timed with CUDA events on the solver's stream
 (max over ranks). `e2e`: the same metric through the reference-facing call
 with host buffers: upload of the state from pinned host memory, the steps,
 and the download of the final state, all inside the timed region.
-Variants: FP64 pull and push, FP32 and FP16 storage (FP32 arithmetic) with
-their L2 velocity/density error against the FP64 run of the same seed.
+Variants: FP64 pull and push; FP32 and FP16 storage (FP32 arithmetic) in
+the AA and pull patterns, each with its L2 velocity/density error against
+the FP64 AA run of the same seed after the same number of steps.
 
 Adjoint (`adjoint` key of the default line): 128^3 Brinkman channel (walls
 on the y and z faces, x periodic, FP32 porosity uniform in [0, 1] from a
@@ -299,25 +300,26 @@ def run_native(args, dist: Dist):
             "gbs": n_fluid * vsteps * v.bytes_per_update / (t / 1e3) / 1e9}
         variants[f"fp64_{pattern}"]["frac"] = variants[f"fp64_{pattern}"]["gbs"] / peak
         v.close()
+    ref = solver(L, flags, "aa", L.F64, f0)  # accuracy reference: FP64, same seed
+    ref.run(args.steps)
     for name, prec in (("fp32", L.F32), ("fp16", L.F16)):
-        # accuracy: same seed and step count as a fresh FP64 run
-        a = solver(L, flags, "aa", L.F64, f0)
-        b = solver(L, flags, "aa", prec, f0)
-        a.run(args.steps)
-        b.run(args.warmup)
-        t = b.run_timed(args.steps - args.warmup) if args.steps > args.warmup else None
-        d = b.compare(a)
-        mlups = n_fluid * (args.steps - args.warmup) / (t / 1e3) / 1e6 if t else None
-        variants[f"{name}_aa"] = {
-            "mlups": mlups, "gbs": mlups * b.bytes_per_update / 1e3 if mlups else None,
-            "l2_rel_err_u": float(np.sqrt(d[0] / d[1])) if d[1] > 0 else None,
-            "l2_rel_err_rho": float(np.sqrt(d[2] / d[3])) if d[3] > 0 else None,
-            "error_after_steps": args.steps}
-        if mlups:
-            variants[f"{name}_aa"]["frac"] = variants[f"{name}_aa"]["gbs"] / peak
-            variants[f"{name}_aa"]["speedup_vs_fp64_aa"] = mlups / (value / dist.world)
-        a.close()
-        b.close()
+        for pattern in ("aa", "pull"):
+            b = solver(L, flags, pattern, prec, f0)
+            b.run(args.warmup)
+            t = b.run_timed(args.steps - args.warmup) if args.steps > args.warmup else None
+            d = b.compare(ref)
+            mlups = n_fluid * (args.steps - args.warmup) / (t / 1e3) / 1e6 if t else None
+            key = f"{name}_{pattern}"
+            variants[key] = {
+                "mlups": mlups, "gbs": mlups * b.bytes_per_update / 1e3 if mlups else None,
+                "l2_rel_err_u": float(np.sqrt(d[0] / d[1])) if d[1] > 0 else None,
+                "l2_rel_err_rho": float(np.sqrt(d[2] / d[3])) if d[3] > 0 else None,
+                "error_after_steps": args.steps}
+            if mlups:
+                variants[key]["frac"] = variants[key]["gbs"] / peak
+                variants[key]["speedup_vs_fp64_aa"] = mlups / (value / dist.world)
+            b.close()
+    ref.close()
 
     # ---- e2e: through the reference-facing call with pinned host buffers
     e2e = run_e2e(L, flags, f0, args.steps, dist)

@@ -71,6 +71,7 @@ struct lbm_solver {
   long long launches;
   size_t dev_bytes;
   int no_shuffle; // reduced precision: never use the shuffle-aligned kernels
+  int no_quad;    // FP16 AA even: never use the four-cell kernel
   void *u_save_next; // adjoint recomputation: momentum output of the next step
   int slab;          // x-slab of a decomposed domain: device planes 0 and nx+1 are ghosts
   int tma;           // FP64 steps use the bulk-copy pipelined kernels (shape in tma_shape)
@@ -554,6 +555,8 @@ static int create_impl(lbm_solver **out, int nx, int ny, int nz, const int *flag
   {
     const char *ns = getenv("LBM_B200_NO_SHUFFLE");
     s->no_shuffle = (ns && ns[0] == '1') ? 1 : 0;
+    const char *nq = getenv("LBM_B200_NO_QUAD");
+    s->no_quad = (nq && nq[0] == '1') ? 1 : 0;
   }
   cudaGetDevice(&s->device);
 
@@ -1057,6 +1060,7 @@ static int launch_one(lbm_solver *s, int *kind_out)
     a.u_save = brink ? (float *)s->u_save_next : nullptr;
     a.c = make_consts2(s);
     a.no_shuffle = s->no_shuffle;
+    a.no_quad = s->no_quad;
     e = launch_step_x2_f32(kind, force, brink, a, s->stream);
   } else {
     StepArgs2<StoreF16> a;
@@ -1068,6 +1072,7 @@ static int launch_one(lbm_solver *s, int *kind_out)
     a.u_save = nullptr;
     a.c = make_consts2(s);
     a.no_shuffle = s->no_shuffle;
+    a.no_quad = s->no_quad;
     e = launch_step_x2_f16(kind, force, brink, a, s->stream);
   }
   if (e != cudaSuccess)

@@ -1,6 +1,8 @@
 // Reduced-precision step kernels: FP32 arithmetic on shifted populations
 // g_d = f_d - w_d, stored as FP32 or as FP16 (scaled by a power of two), two
 // cells per thread (lbm_step_x2.cuh). Multiply-add contraction is allowed.
+#include <type_traits>
+
 #include "lbm_internal.h"
 #include "lbm_step_x2.cuh"
 #include "lbm_step_x2s.cuh"
@@ -8,11 +10,19 @@
 namespace lbm {
 
 // The shuffle-aligned kernel serves the shifted patterns when nz is a
-// multiple of 64; AA even (all accesses local) and other extents use the
-// generic two-cell kernel.
+// multiple of 64; AA even in FP16 storage takes the four-cell kernel; the
+// rest uses the generic two-cell kernel.
 template <class ST, int KIND, bool FORCE, bool BRINK>
 static cudaError_t go(const StepArgs2<ST> &a, dim3 grid, dim3 block, cudaStream_t st)
 {
+  if constexpr (std::is_same<ST, StoreF16>::value && KIND == kAAEvenStep && !BRINK) {
+    if (a.g.pz % 4 == 0 && !a.no_quad) {
+      dim3 qg, qb;
+      quad_launch_shape(a.g, qg, qb);
+      step_kernel_even_quad<FORCE><<<qg, qb, 0, st>>>(a);
+      return cudaGetLastError();
+    }
+  }
   if (KIND != kAAEvenStep && a.g.nz % 64 == 0 && !a.no_shuffle) {
     dim3 sg, sb;
     shuffle_launch_shape(a.g, sg, sb);

@@ -106,6 +106,28 @@ def test_shuffle_aligned_kernels_equal_generic_pair_kernels(precision, per):
         assert np.array_equal(outs[0], outs[1]), pattern
 
 
+@pytest.mark.parametrize("dims", [(9, 11, 128), (7, 6, 13), (5, 8, 30)])
+@pytest.mark.parametrize("per", [(1, 0, 0), (1, 1, 1), (0, 1, 1)])
+def test_fp16_four_cell_even_kernel_equals_pair_kernel(monkeypatch, dims, per):
+    """FP16 AA even steps run the four-cells-per-thread kernel; it collides
+    the two pairs with the pair kernel's arithmetic, so the states agree bit
+    for bit with LBM_B200_NO_QUAD=1 (ragged nz, walls, force, odd and even
+    step counts)."""
+    rng = np.random.default_rng(sum(dims))
+    flags = _random_walls(rng, dims, per)
+    f0 = L.perturbed_equilibrium(flags, seed=5, amplitude=2e-3)
+    for steps in (1, 4, 7):
+        outs = []
+        for no_quad in ("0", "1"):
+            monkeypatch.setenv("LBM_B200_NO_QUAD", no_quad)
+            with L.Solver(flags, per, "aa", L.F16) as s:
+                s.set_params(1.3, 3 / 16, 1e-5, True)
+                s.set_state(f0)
+                s.run(steps)
+                outs.append(s.get_state())
+        assert np.array_equal(outs[0], outs[1]), steps
+
+
 @pytest.mark.parametrize("per", [(1, 0, 0), (1, 1, 1)])
 def test_shuffle_aligned_kernels_track_the_oracle(oracle, per):
     import oracle as O
