@@ -59,8 +59,19 @@ template <class ST> struct StepArgs {
 #ifndef LBM_MINB_LP
 #define LBM_MINB_LP 4
 #endif
+// Per kind for FP64, from a sweep on the 256^3 porous channel (B200): the
+// AA odd step is fastest at 7 CTAs per SM (72 registers), pull at 5 (96),
+// AA even and push at 6 (80); 8 spills.
+#ifndef LBM_MINB_F64_ODD
+#define LBM_MINB_F64_ODD 7
+#endif
+#ifndef LBM_MINB_F64_PULL
+#define LBM_MINB_F64_PULL 5
+#endif
 template <class ST, int KIND> struct StepOccupancy {
-  static constexpr int value = sizeof(typename ST::S) == 8 ? LBM_MINB_F64 : LBM_MINB_LP;
+  static constexpr int value = sizeof(typename ST::S) != 8 ? LBM_MINB_LP
+      : KIND == kAAOddStep ? LBM_MINB_F64_ODD
+      : KIND == kPullStep ? LBM_MINB_F64_PULL : LBM_MINB_F64;
 };
 
 // Read-only loads of the two-lattice patterns may take the non-coherent

@@ -126,12 +126,22 @@ template <class ST> struct StepArgs2 {
   int no_quad;    // host-side switch: AA even in FP16 storage on the two-cell kernel
 };
 
+// Minimum resident CTAs per SM of the pair kernels, per storage type and
+// kind, from a sweep of the shuffle-aligned kernels on the 256^3 porous
+// channel (B200): pull 8, AA odd 7 (FP16) or 4 (FP32), everything else 6.
+// The generic kernel keeps 6 for AA odd (at 7 it spills).
 #ifndef LBM_MINB_X2
 #define LBM_MINB_X2 6
 #endif
+template <class ST, int KIND, bool SHUFFLE> struct PairOccupancy {
+  static constexpr bool kHalf = sizeof(typename ST::S) == 2;
+  static constexpr int value = KIND == kPullStep ? 8
+      : (KIND == kAAOddStep && SHUFFLE) ? (kHalf ? 7 : 4) : LBM_MINB_X2;
+};
 
 template <class ST, int KIND, bool FORCE, bool BRINK>
-__global__ void __launch_bounds__(kStepThreads, LBM_MINB_X2) step_kernel_x2(StepArgs2<ST> a)
+__global__ void __launch_bounds__(kStepThreads, (PairOccupancy<ST, KIND, false>::value))
+    step_kernel_x2(StepArgs2<ST> a)
 {
   using PT = PairOf<ST>;
   using S = typename PT::S;

@@ -29,7 +29,8 @@ namespace lbm {
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
 template <class ST, int KIND, bool FORCE, bool BRINK>
-__global__ void __launch_bounds__(kStepThreads, LBM_MINB_X2) step_kernel_x2s(StepArgs2<ST> a)
+__global__ void __launch_bounds__(kStepThreads, (PairOccupancy<ST, KIND, true>::value))
+    step_kernel_x2s(StepArgs2<ST> a)
 {
   using PT = PairOf<ST>;
   using S = typename PT::S;
