@@ -117,6 +117,21 @@ int lbm_get_state(lbm_solver *s, double *f);
 int lbm_set_state_padded(lbm_solver *s, const void *pdfs, int elem_size, int ref_orientation);
 int lbm_get_state_padded(lbm_solver *s, void *pdfs, int elem_size, int ref_orientation);
 
+/* Zou-He pressure boundary (src/lbm.c:676-785, kernelComputeBoundaryConditions,
+ * which LBM-Bench defines but never calls). With on = 1, after every step
+ * the cells flagged 2 (LAT_CELL_INLET) on the plane x = 0 get the five
+ * populations entering from x - 1 (E, NE, SE, TE, BE) that give them density
+ * rho_in, and the cells flagged 4 (LAT_CELL_OUTLET) on x = nx-1 the five
+ * entering from x + 1 (W, NW, SW, TW, BW) for rho_out; as in the reference
+ * only the interior rows 1 <= y <= ny-2, 1 <= z <= nz-2 take part. The
+ * FP64 state equals the reference's pull and push kernels each followed by
+ * that function (the reference's AA kernel can only apply it after a pair
+ * of steps; here it follows every step of every pattern). x should not be
+ * periodic. LBM_ERR_STATE if the flags of lbm_create had no such cells; not
+ * available on slab solvers or with lbm_adjoint_gradient. on = 0 turns it
+ * off. */
+int lbm_set_pressure_bc(lbm_solver *s, double rho_in, double rho_out, int on);
+
 /* Halo exchange of slab solvers. lbm_halo_needs tells which exchanges the
  * next step takes (LBM_HALO_BEFORE: pull, AA odd; LBM_HALO_AFTER: push, AA
  * odd; none for an AA even step). lbm_halo_pack writes the two messages

@@ -27,6 +27,13 @@ cudaError_t launch_step_x2_f32(int kind, bool force, bool brink, const StepArgs2
 cudaError_t launch_step_x2_f16(int kind, bool force, bool brink, const StepArgs2<StoreF16> &a,
     cudaStream_t st);
 
+// Zou-He pressure boundary on the state after a step (lbm_step_f64.cu):
+// marks is [2][ny][nz] (caller's box; 0 = inlet plane x = 0, 1 = outlet
+// plane x = nx - 1), nonzero where the boundary applies.
+cudaError_t launch_pressure_bc(int precision, const Grid &g, const UserBox &u, int orient,
+    void *state, const uint32_t *mask, const uint8_t *marks, double rho_in, double rho_out,
+    float scale, cudaStream_t st);
+
 // Adjoint launchers (lbm_adjoint.cu): one reverse step; seed of lambda at
 // the final state for the outlet objective on device plane x = xo.
 cudaError_t launch_adjoint_step_f64(const AdjArgs<double> &a, cudaStream_t st);

@@ -78,6 +78,9 @@ struct lbm_solver {
   int tma_groups;    // consumer groups of 8 warps per CTA
   TmaShape tma_shape;
   unsigned int *dev_err; // set by kernels whose bounded waits ran out
+  uint8_t *bc_marks;     // [2][ny][nz]: inlet / outlet cells of the pressure boundary, or NULL
+  int bc_on;
+  double rho_in, rho_out;
 };
 
 extern "C" const char *lbm_last_error(void) { return g_err; }
@@ -491,6 +494,7 @@ static void free_all(lbm_solver *s)
   cudaFree(s->pstaging);
   cudaFree(s->red);
   cudaFree(s->dev_err);
+  cudaFree(s->bc_marks);
   if (s->ev[0])
     cudaEventDestroy(s->ev[0]);
   if (s->ev[1])
@@ -663,6 +667,26 @@ static int create_impl(lbm_solver **out, int nx, int ny, int nz, const int *flag
       s->tma_shape.stages -= s->tma_shape.stages % s->tma_groups;
       s->tma = s->tma_shape.stages >= s->tma_groups;
       s->tma_shape.blocks = s->tma_shape.ntiles < sms ? s->tma_shape.ntiles : sms;
+    }
+  }
+
+  {
+    // cells of the Zou-He pressure boundary (src/lbm.c:693-700): flag 2 on
+    // x = 0 and flag 4 on x = nx - 1, on the interior rows 1..ny-2, 1..nz-2
+    std::vector<uint8_t> marks((size_t)2 * ny * nz, 0);
+    bool any = false;
+    for (int side = 0; side < 2 && !slab; ++side)
+      for (int y = 1; y < ny - 1; ++y)
+        for (int z = 1; z < nz - 1; ++z) {
+          const int x = side ? nx - 1 : 0;
+          if (flags[((long long)z * ny + y) * nx + x] == (side ? 4 : 2)) {
+            marks[((size_t)side * ny + y) * nz + z] = 1;
+            any = true;
+          }
+        }
+    if (any) {
+      TRY(dev_alloc(s, (void **)&s->bc_marks, marks.size(), "the pressure-boundary marks"));
+      TRYC(cudaMemcpy(s->bc_marks, marks.data(), marks.size(), cudaMemcpyHostToDevice));
     }
   }
 
@@ -1083,6 +1107,33 @@ static int launch_one(lbm_solver *s, int *kind_out)
   s->launches++;
   if (kind_out)
     *kind_out = kind;
+  if (s->bc_on) {
+    e = launch_pressure_bc(s->precision, s->g, s->ub, orientation(s), (void *)state_ptr(s),
+        s->mask, s->bc_marks, s->rho_in, s->rho_out,
+        (float)(s->precision == LBM_F16 ? s->fp16_scale : 1.0), s->stream);
+    if (e != cudaSuccess)
+      return fail(LBM_ERR_CUDA, "pressure boundary launch failed: %s", cudaGetErrorString(e));
+  }
+  return LBM_OK;
+}
+
+extern "C" int lbm_set_pressure_bc(lbm_solver *s, double rho_in, double rho_out, int on)
+{
+  if (!s)
+    return fail(LBM_ERR_ARG, "lbm_set_pressure_bc: NULL solver");
+  if (!on) {
+    s->bc_on = 0;
+    return LBM_OK;
+  }
+  if (!(rho_in > 0.0) || !(rho_out > 0.0) || !isfinite(rho_in) || !isfinite(rho_out))
+    return fail(LBM_ERR_ARG, "lbm_set_pressure_bc: densities %g, %g must be positive", rho_in,
+        rho_out);
+  if (!s->bc_marks)
+    return fail(LBM_ERR_STATE, "lbm_set_pressure_bc: the flags have no inlet (2) cells on x = 0 "
+        "or outlet (4) cells on x = nx-1 inside the y/z walls");
+  s->rho_in = rho_in;
+  s->rho_out = rho_out;
+  s->bc_on = 1;
   return LBM_OK;
 }
 
@@ -1664,6 +1715,8 @@ extern "C" int lbm_adjoint_gradient(lbm_solver *s, int steps, int checkpoint_eve
     return fail(LBM_ERR_ARG, "lbm_adjoint_gradient: needs an AA solver");
   if (s->slab)
     return fail(LBM_ERR_ARG, "lbm_adjoint_gradient: not available on slab solvers");
+  if (s->bc_on)
+    return fail(LBM_ERR_ARG, "lbm_adjoint_gradient: not available with the pressure boundary");
   if (s->precision == LBM_F16)
     return fail(LBM_ERR_ARG, "lbm_adjoint_gradient: FP16 storage is not supported (FP64/FP32)");
   if (!s->porosity || s->alpha == 0.0)

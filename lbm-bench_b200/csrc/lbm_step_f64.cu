@@ -70,6 +70,102 @@ cudaError_t launch_step_tma_f64(int kind, bool force, const TmaArgs<StoreF64> &a
   return cudaErrorInvalidValue;
 }
 
+// Zou-He pressure boundary (src/lbm.c:676-785, kernelComputeBoundaryConditions),
+// applied to the state after a step, one thread per (y, z) of the inlet
+// plane (blockIdx.z = 0, x = 0) or the outlet plane (1, x = nx - 1) where
+// `marks` flags a cell. Populations are read and written through the
+// orientation of the current state, so the kernel serves every pattern.
+// It fixes the five populations entering across the x face from the
+// outside - E, NE, SE, TE, BE at the inlet, W, NW, SW, TW, BW at the outlet
+// - from the fourteen known ones so that the cell's density is rho_in or
+// rho_out. The arithmetic is the reference's, operation for operation and
+// in FP64 (this unit has no multiply-add contraction), so the FP64 state is
+// bit-identical to the reference's pull and push kernels followed by its
+// boundary pass; shifted storage adds and removes w_d around it.
+template <class ST>
+__global__ void pressure_bc_kernel(Grid g, UserBox u, int orient, typename ST::S *state,
+    const uint32_t *__restrict__ mask, const uint8_t *__restrict__ marks, double rho_in,
+    double rho_out, float scale, float inv_scale)
+{
+  using V = typename ST::V;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int side = blockIdx.z;
+  if (z >= u.nz || y >= u.ny || !marks[((size_t)side * u.ny + y) * u.nz + z])
+    return;
+  const int x = side ? u.nx - 1 : 0;
+  const uint32_t cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
+  const uint32_t m = mask[cell];
+  if (m & kSolidBit)
+    return;
+  const Offs nb = make_offs(g, x + u.ox, y + u.oy, z + u.oz);
+  auto at = [&](int d) {
+    int p;
+    uint32_t c;
+    state_slot(orient, d, m, cell, nb, p, c);
+    return state + (size_t)p * g.plane + c;
+  };
+  auto wgt = [](int d) {
+    const int c = wclass(d);
+    return c == 0 ? 1.0 / 3.0 : c == 1 ? 1.0 / 18.0 : 1.0 / 36.0;
+  };
+  auto get = [&](int d) {
+    double v = (double)ST::decode(*at(d), (V)inv_scale);
+    return ST::kShifted ? v + wgt(d) : v;
+  };
+  auto put = [&](int d, double v) {
+    if (ST::kShifted)
+      v -= wgt(d);
+    ST::store(at(d), (V)v, (V)scale);
+  };
+  const double third = 1.0 / 3.0, quarter = 1.0 / 4.0, sixth = 1.0 / 6.0;
+  const double fN = get(dN), fS = get(dS), fT = get(dT), fB = get(dB);
+  const double rest = get(dC) + (fT + fB + fS + fN) + (get(dTS) + get(dBS) + get(dTN) + get(dBN));
+  if (side == 0) {
+    const double dens = rho_in;
+    const double fW = get(dW), fSW = get(dSW), fNW = get(dNW), fTW = get(dTW), fBW = get(dBW);
+    const double ux = 1.0 - (rest + 2.0 * (fSW + fTW + fW + fBW + fNW)) * (1.0 / rho_in);
+    const double ind = sixth * dens * ux;
+    put(dE, fW + third * dens * ux);
+    put(dNE, fSW - quarter * (fN - fS) + ind);
+    put(dSE, fNW + quarter * (fN - fS) + ind);
+    put(dTE, fBW - quarter * (fT - fB) + ind);
+    put(dBE, fTW + quarter * (fT - fB) + ind);
+  } else {
+    const double dens = rho_out;
+    const double fE = get(dE), fNE = get(dNE), fSE = get(dSE), fTE = get(dTE), fBE = get(dBE);
+    const double ux = -1.0 + (rest + 2.0 * (fNE + fBE + fE + fTE + fSE)) * (1.0 / rho_out);
+    const double ind = sixth * dens * ux;
+    put(dW, fE - third * dens * ux);
+    put(dSW, fNE + quarter * (fN - fS) - ind);
+    put(dNW, fSE - quarter * (fN - fS) - ind);
+    put(dBW, fTE + quarter * (fT - fB) - ind);
+    put(dTW, fBE - quarter * (fT - fB) - ind);
+  }
+}
+
+cudaError_t launch_pressure_bc(int precision, const Grid &g, const UserBox &u, int orient,
+    void *state, const uint32_t *mask, const uint8_t *marks, double rho_in, double rho_out,
+    float scale, cudaStream_t st)
+{
+  dim3 block(32, 4, 1);
+  dim3 grid((u.nz + 31) / 32, (u.ny + 3) / 4, 2);
+  switch (precision) {
+  case kF64:
+    pressure_bc_kernel<StoreF64><<<grid, block, 0, st>>>(g, u, orient, (double *)state, mask,
+        marks, rho_in, rho_out, 1.f, 1.f);
+    break;
+  case kF32:
+    pressure_bc_kernel<StoreF32><<<grid, block, 0, st>>>(g, u, orient, (float *)state, mask,
+        marks, rho_in, rho_out, 1.f, 1.f);
+    break;
+  default:
+    pressure_bc_kernel<StoreF16><<<grid, block, 0, st>>>(g, u, orient, (__half *)state, mask,
+        marks, rho_in, rho_out, scale, 1.f / scale);
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_step_f64(int kind, bool force, bool brink, const StepArgs<StoreF64> &a,
     dim3 grid, dim3 block, cudaStream_t st)
 {

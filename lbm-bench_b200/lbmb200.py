@@ -50,6 +50,8 @@ _SIGNATURES = [
     ("lbm_create_slab", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, ctypes.c_int]),
+    ("lbm_set_pressure_bc", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_int]),
     ("lbm_halo_bytes", ctypes.c_size_t, [_vp]),
     ("lbm_halo_needs", ctypes.c_int, [_vp]),
     ("lbm_halo_shifted", ctypes.c_int, [_vp]),
@@ -233,6 +235,12 @@ class Solver:
     # -- configuration -----------------------------------------------------
     def set_params(self, omega=1.0, lam=1.0 / 12.0, xforce=1e-5, force_on=False):
         _check(lib().lbm_set_params(self._h, omega, lam, xforce, int(force_on)))
+
+    def set_pressure_bc(self, rho_in: float, rho_out: float, on: bool = True):
+        """Zou-He pressure boundary after every step (lbm_set_pressure_bc):
+        inlet cells (flag 2) on x = 0 at rho_in, outlet cells (flag 4) on
+        x = nx-1 at rho_out."""
+        _check(lib().lbm_set_pressure_bc(self._h, rho_in, rho_out, int(on)))
 
     def set_fp16_scale(self, scale: float):
         _check(lib().lbm_set_fp16_scale(self._h, scale))

@@ -226,9 +226,74 @@ static void step(const Grid *g, const Params *p, const float *porosity, const do
   }
 }
 
+/* Zou-He pressure boundary after a step (src/lbm.c:676-785,
+ * kernelComputeBoundaryConditions), in the receiver view: on the interior
+ * rows (1 <= y <= ny-2, 1 <= z <= nz-2) of plane x = 0 every cell flagged 2
+ * (LAT_CELL_INLET) gets the five populations that enter from x - 1 (E, NE,
+ * SE, TE, BE) chosen so that its density is rho_in; on plane x = nx-1 every
+ * cell flagged 4 (LAT_CELL_OUTLET) gets W, NW, SW, TW, BW for rho_out. The
+ * operations are the reference's, in its order. */
+enum { dN = 0, dS, dE, dW, dNE, dSE, dNW, dSW, dT, dTN, dTE, dTW, dTS, dB, dBS, dBN, dBW, dBE, dC };
+
+static void pressure_bc(const Grid *g, const int *flags, double rho_in, double rho_out,
+    double *f)
+{
+  const long long nc = g->ncells;
+  const double third = 1.0 / 3.0, quarter = 1.0 / 4.0, sixth = 1.0 / 6.0;
+  const double in_inv = 1.0 / rho_in, out_inv = 1.0 / rho_out;
+  for (int z = 1; z < g->nz - 1; ++z)
+    for (int y = 1; y < g->ny - 1; ++y) {
+      for (int side = 0; side < 2; ++side) {
+        const int x = side ? g->nx - 1 : 0;
+        if (flags[((long long)z * g->ny + y) * g->nx + x] != (side ? 4 : 2))
+          continue;
+        double *p = f + cidx(g, x, y, z);
+#define F_(d) p[(long long)(d) * nc]
+        const double rest = F_(dC) + (F_(dT) + F_(dB) + F_(dS) + F_(dN)) +
+            (F_(dTS) + F_(dBS) + F_(dTN) + F_(dBN));
+        if (!side) {
+          const double dens = rho_in;
+          const double ux = 1.0 -
+              (rest + 2.0 * (F_(dSW) + F_(dTW) + F_(dW) + F_(dBW) + F_(dNW))) * in_inv;
+          const double ind = sixth * dens * ux;
+          F_(dE)  = F_(dW) + third * dens * ux;
+          F_(dNE) = F_(dSW) - quarter * (F_(dN) - F_(dS)) + ind;
+          F_(dSE) = F_(dNW) + quarter * (F_(dN) - F_(dS)) + ind;
+          F_(dTE) = F_(dBW) - quarter * (F_(dT) - F_(dB)) + ind;
+          F_(dBE) = F_(dTW) + quarter * (F_(dT) - F_(dB)) + ind;
+        } else {
+          const double dens = rho_out;
+          const double ux = -1.0 +
+              (rest + 2.0 * (F_(dNE) + F_(dBE) + F_(dE) + F_(dTE) + F_(dSE))) * out_inv;
+          const double ind = sixth * dens * ux;
+          F_(dW)  = F_(dE) - third * dens * ux;
+          F_(dSW) = F_(dNE) + quarter * (F_(dN) - F_(dS)) - ind;
+          F_(dNW) = F_(dSE) - quarter * (F_(dN) - F_(dS)) - ind;
+          F_(dBW) = F_(dTE) + quarter * (F_(dT) - F_(dB)) - ind;
+          F_(dTW) = F_(dBE) - quarter * (F_(dT) - F_(dB)) - ind;
+        }
+#undef F_
+      }
+    }
+}
+
+static int run_common_bc(int nx, int ny, int nz, const int *flags, int px, int py, int pz,
+    double omega, double lambda, double xforce, int force_on, double alpha,
+    const float *porosity, int steps, const double *f_in, double *f_out, int bc_every,
+    double rho_in, double rho_out);
+
 static int run_common(int nx, int ny, int nz, const int *flags, int px, int py, int pz,
     double omega, double lambda, double xforce, int force_on, double alpha,
     const float *porosity, int steps, const double *f_in, double *f_out)
+{
+  return run_common_bc(nx, ny, nz, flags, px, py, pz, omega, lambda, xforce, force_on, alpha,
+      porosity, steps, f_in, f_out, 0, 1.0, 1.0);
+}
+
+static int run_common_bc(int nx, int ny, int nz, const int *flags, int px, int py, int pz,
+    double omega, double lambda, double xforce, int force_on, double alpha,
+    const float *porosity, int steps, const double *f_in, double *f_out, int bc_every,
+    double rho_in, double rho_out)
 {
   Grid g;
   if (grid_init(&g, nx, ny, nz, flags, px, py, pz) != 0 || steps < 0 || !f_in || !f_out)
@@ -250,6 +315,8 @@ static int run_common(int nx, int ny, int nz, const int *flags, int px, int py, 
     double *t = a;
     a         = b;
     b         = t;
+    if (bc_every > 0 && (s + 1) % bc_every == 0)
+      pressure_bc(&g, flags, rho_in, rho_out, a);
   }
   memcpy(f_out, a, bytes);
   free(a);
@@ -418,4 +485,14 @@ int orc_adjoint_brinkman(int nx, int ny, int nz, const int *flags, int px, int p
   free(lam2);
   free(g.fluid);
   return 0;
+}
+
+int orc_run_pressure(int nx, int ny, int nz, const int *flags, int px, int py, int pz,
+    double omega, double lambda, double xforce, int force_on, double rho_in, double rho_out,
+    int bc_every, int steps, const double *f_in, double *f_out)
+{
+  if (bc_every < 1 || !(rho_in > 0.0) || !(rho_out > 0.0))
+    return -1;
+  return run_common_bc(nx, ny, nz, flags, px, py, pz, omega, lambda, xforce, force_on, 0.0, NULL,
+      steps, f_in, f_out, bc_every, rho_in, rho_out);
 }

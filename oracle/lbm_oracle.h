@@ -31,6 +31,14 @@ int orc_run_brinkman(int nx, int ny, int nz, const int *flags, int px, int py, i
     double omega, double lambda, double xforce, double alpha, const float *porosity, int steps,
     const double *f_in, double *f_out);
 
+/* orc_run with the Zou-He pressure boundary of src/lbm.c:676-785 applied
+ * after every bc_every-th step: cells flagged 2 on plane x = 0 (inlet,
+ * density rho_in) and 4 on plane x = nx-1 (outlet, rho_out), interior y/z
+ * rows only. Returns 0, or -1 on bad input. */
+int orc_run_pressure(int nx, int ny, int nz, const int *flags, int px, int py, int pz,
+    double omega, double lambda, double xforce, int force_on, double rho_in, double rho_out,
+    int bc_every, int steps, const double *f_in, double *f_out);
+
 /* Objective J = mean over the fluid cells of plane x = nx-1 of the x
  * momentum sum_d c_dx f_d. */
 double orc_objective(int nx, int ny, int nz, const int *flags, const double *f);

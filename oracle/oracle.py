@@ -68,6 +68,10 @@ class Oracle:
         L.orc_run_brinkman.restype = ctypes.c_int
         L.orc_run_brinkman.argtypes = [ctypes.c_int] * 3 + [_ip] + [ctypes.c_int] * 3 + \
             [ctypes.c_double] * 4 + [_fp, ctypes.c_int, _dp, _dp]
+        L.orc_run_pressure.restype = ctypes.c_int
+        L.orc_run_pressure.argtypes = [ctypes.c_int] * 3 + [_ip] + [ctypes.c_int] * 3 + \
+            [ctypes.c_double] * 3 + [ctypes.c_int] + [ctypes.c_double] * 2 + \
+            [ctypes.c_int, ctypes.c_int, _dp, _dp]
         L.orc_objective.restype = ctypes.c_double
         L.orc_objective.argtypes = [ctypes.c_int] * 3 + [_ip, _dp]
         L.orc_adjoint_brinkman.restype = ctypes.c_int
@@ -97,6 +101,21 @@ class Oracle:
                                        _ptr(f_in, _dp), _ptr(out, _dp))
         if rc != 0:
             raise RuntimeError("orc_run_brinkman failed")
+        return out
+
+    def run_pressure(self, flags, periodic, f_in, steps, omega, lam, xforce, force_on,
+                     rho_in, rho_out, bc_every=1):
+        """orc_run with the Zou-He pressure boundary after every bc_every-th
+        step (inlet flag 2 on x = 0, outlet flag 4 on x = nx-1)."""
+        nz, ny, nx = flags.shape
+        flags = np.ascontiguousarray(flags, dtype=np.int32)
+        f_in = np.ascontiguousarray(f_in, dtype=np.float64)
+        out = np.empty_like(f_in)
+        rc = self.lib.orc_run_pressure(nx, ny, nz, _ptr(flags, _ip), *[int(p) for p in periodic],
+                                       omega, lam, xforce, int(force_on), rho_in, rho_out,
+                                       bc_every, steps, _ptr(f_in, _dp), _ptr(out, _dp))
+        if rc != 0:
+            raise RuntimeError("orc_run_pressure failed")
         return out
 
     def objective(self, flags, f):
@@ -145,6 +164,9 @@ class Reference:
         L.ref_run.argtypes = [ctypes.c_char_p] + [ctypes.c_int] * 3 + [_ip] + \
             [ctypes.c_int] * 3 + [ctypes.c_double] * 2 + [ctypes.c_int, ctypes.c_int, _dp, _dp,
                                                           _dp, _ip, _ip]
+        L.ref_run_pressure.restype = ctypes.c_int
+        L.ref_run_pressure.argtypes = [ctypes.c_char_p] + [ctypes.c_int] * 3 + [_ip] + \
+            [ctypes.c_int] * 3 + [ctypes.c_double] * 4 + [ctypes.c_int, _dp, _dp]
         L.ref_verify.restype = ctypes.c_int
         L.ref_verify.argtypes = [ctypes.c_int] * 3 + [_ip] + [ctypes.c_int] * 3 + \
             [ctypes.c_double] * 2 + [_dp, _dp]
@@ -189,6 +211,22 @@ class Reference:
         if rc != 0:
             raise KeyError(kernel)
         return out, dur.value, it.value, nbb.value
+
+    def run_pressure(self, kernel, flags, periodic, f_in, calls, omega, xforce, rho_in,
+                     rho_out):
+        """`calls` kd->Kernel calls of one iteration (one step for pull and
+        push, two for AA), each followed by the reference's
+        kernelComputeBoundaryConditions. Returns the final state."""
+        nz, ny, nx = flags.shape
+        flags = np.ascontiguousarray(flags, dtype=np.int32)
+        f_in = np.ascontiguousarray(f_in, dtype=np.float64)
+        out = np.zeros_like(f_in)
+        rc = self.lib.ref_run_pressure(kernel.encode(), nx, ny, nz, _ptr(flags, _ip),
+                                       *[int(p) for p in periodic], omega, xforce, rho_in,
+                                       rho_out, calls, _ptr(f_in, _dp), _ptr(out, _dp))
+        if rc != 0:
+            raise KeyError(kernel)
+        return out
 
     def verify(self, flags, periodic, f, omega, xforce) -> float:
         nz, ny, nx = flags.shape

@@ -171,6 +171,87 @@ int ref_run(const char *name, int nx, int ny, int nz, const int *flags, int px, 
   return 0;
 }
 
+/* ref_run with the reference's Zou-He pressure boundary
+ * (kernelComputeBoundaryConditions, src/lbm.c:676-785) applied after every
+ * kd->Kernel call of one iteration: one step for pull and push, two for AA
+ * (src/kernel_aa_soa.c:36 runs iterations in pairs). `calls` kernel calls
+ * are made. flags carry 2 (inlet, x = 0) and 4 (outlet, x = nx-1). */
+int ref_run_pressure(const char *name, int nx, int ny, int nz, const int *flags, int px, int py,
+    int pz, double omega, double xforce, double rho_in, double rho_out, int calls,
+    const double *pdfs_in, double *pdfs_out)
+{
+  KernelFunctionsType *kf = NULL;
+  for (int j = 0; j < G_N_KERNELS; ++j)
+    if (!strcasecmp(name, GKernels[j].Name)) {
+      kf = &GKernels[j];
+      break;
+    }
+  if (kf == NULL)
+    return -1;
+  LatticeDescType ld;
+  memset(&ld, 0, sizeof(ld));
+  ld.Dims[0]   = nx;
+  ld.Dims[1]   = ny;
+  ld.Dims[2]   = nz;
+  ld.nCells    = nx * ny * nz;
+  ld.PeriodicX = px;
+  ld.PeriodicY = py;
+  ld.PeriodicZ = pz;
+  ld.Name      = "harness";
+  ld.Lattice   = (LatticeType *)malloc(sizeof(LatticeType) * (size_t)ld.nCells);
+  memcpy(ld.Lattice, flags, sizeof(LatticeType) * (size_t)ld.nCells);
+  for (int i = 0; i < ld.nCells; ++i) {
+    if (flags[i] == LAT_CELL_OBSTACLE)
+      ld.nObst++;
+    else
+      ld.nFluid++;
+    ld.nInlet += flags[i] == LAT_CELL_INLET;
+    ld.nOutlet += flags[i] == LAT_CELL_OUTLET;
+  }
+  CaseDataType cd;
+  cd.Omega             = (PdfType)omega;
+  cd.RhoIn             = (PdfType)rho_in;
+  cd.RhoOut            = (PdfType)rho_out;
+  cd.XForce            = (PdfType)xforce;
+  cd.MaxIterations     = 1;
+  cd.StatisticsModulus = 100;
+  KernelDataType *kd = NULL;
+  kf->Init(&ld, &kd, &cd);
+  PdfType pdfs[N_D3Q19];
+  for (int x = 0; x < nx; ++x)
+    for (int y = 0; y < ny; ++y)
+      for (int z = 0; z < nz; ++z) {
+        if (flags[latticeIndex(ld.Dims, x, y, z)] == LAT_CELL_OBSTACLE)
+          continue;
+        for (int d = 0; d < N_D3Q19; ++d)
+          pdfs[d] = (PdfType)pdfs_in[(long long)d * ld.nCells + dense_index(nx, ny, nz, x, y, z)];
+        kd->SetNode(kd, x, y, z, pdfs);
+      }
+  for (int c = 0; c < calls; ++c) {
+    kd->Kernel(&ld, kd, &cd);
+    // pull and push start every call from Pdfs[0] (src/kernel_pull_soa.c:35-36):
+    // make the lattice the call ended in the next call's source
+    if (kd->PdfsActive != kd->Pdfs[0]) {
+      PdfType *t = kd->Pdfs[0];
+      kd->Pdfs[0] = kd->Pdfs[1];
+      kd->Pdfs[1] = t;
+    }
+    kernelComputeBoundaryConditions(kd, &ld, &cd);
+  }
+  for (int x = 0; x < nx; ++x)
+    for (int y = 0; y < ny; ++y)
+      for (int z = 0; z < nz; ++z) {
+        if (flags[latticeIndex(ld.Dims, x, y, z)] == LAT_CELL_OBSTACLE)
+          continue;
+        kd->GetNode(kd, x, y, z, pdfs);
+        for (int d = 0; d < N_D3Q19; ++d)
+          pdfs_out[(long long)d * ld.nCells + dense_index(nx, ny, nz, x, y, z)] = (double)pdfs[d];
+      }
+  kf->Deinit(&ld, &kd);
+  free(ld.Lattice);
+  return 0;
+}
+
 /* The reference's Poiseuille check (src/lbm.c:964-1023) on a state supplied
  * by the caller: the state is injected into an AA kernel's lattice (natural
  * orientation, Iteration = -1) and kernelVerify is called on it. */

@@ -11,7 +11,9 @@ For every case the script
     and blocked variants for the first cases) and checks they agree bit for
     bit,
   * records the SHA-256 of the final state over fluid cells and some totals.
-It also records the reference's Poiseuille verification (-V) result.
+It also records the reference's Poiseuille verification (-V) result, and
+two pressure-driven channels run with the reference's Zou-He boundary pass
+after every pull and push step.
 
 Usage: python tests/golden/make_golden.py
 """
@@ -105,6 +107,57 @@ def run_case(name, geo, dims, pin, omega, lam, xforce, force, steps, seed, varia
     return case, flags
 
 
+def inlet_outlet_flags(dims, solid, seed):
+    """Channel (walls on the y and z faces) with inlet cells (2) on x = 0
+    and outlet cells (4) on x = nx-1, plus random solid cells inside."""
+    nx, ny, nz = dims
+    rng = np.random.default_rng(seed)
+    flags = np.ones((nz, ny, nx), dtype=np.int32)
+    flags[rng.uniform(size=flags.shape) < solid] = 0
+    flags[:, :, 0] = 2
+    flags[:, :, -1] = 4
+    flags[:, [0, -1], :] = 0
+    flags[[0, -1], :, :] = 0
+    return flags
+
+
+PRESSURE_CASES = [
+    # name, dims, solid, seed, omega, lambda, xforce, force, steps, rho_in, rho_out, variant
+    ("pressure_channel", (12, 9, 8), 0.0, 31, 1.25, 3 / 16, 0.0, 0, 30, 1.005, 0.995,
+     "verify_l316"),
+    ("pressure_porous", (16, 10, 10), 0.15, 32, 1.1, 1 / 12, 1e-6, 1, 12, 1.002, 0.999,
+     "verify"),
+]
+
+
+def run_pressure_case(name, dims, solid, seed, omega, lam, xforce, force, steps, rho_in,
+                      rho_out, variant, arrays):
+    """The reference's pull and push kernels, one step per kd->Kernel call,
+    each followed by its Zou-He pass kernelComputeBoundaryConditions
+    (src/lbm.c:676-785); they must agree bit for bit."""
+    ref = O.Reference(variant)
+    flags = inlet_outlet_flags(dims, solid, seed)
+    f0 = O.perturbed_state(flags, seed)
+    per = (0, 0, 0)
+    outs = {k: ref.run_pressure(k, flags, per, f0, steps, omega, xforce, rho_in, rho_out)
+            for k in ("pull-soa", "push-soa")}
+    m = O.fluid_mask(flags)
+    assert np.array_equal(outs["pull-soa"][:, m], outs["push-soa"][:, m]), name
+    base = outs["pull-soa"]
+    rho, ux, uy, uz = O.moments(base, flags)
+    arrays[f"{name}_flags"] = flags.astype(np.int8)
+    return {
+        "name": name, "geometry": "stored", "dims": list(dims), "periodic_in": [0, 0, 0],
+        "periodic": list(per), "omega": omega, "lambda": lam, "xforce": xforce,
+        "force_on": force, "steps": steps, "seed": seed, "amp": 1e-4, "reference_build": variant,
+        "kernels_agreeing": ["pull-soa", "push-soa"], "n_fluid": int(m.sum()),
+        "flags_key": f"{name}_flags", "pressure": {"rho_in": rho_in, "rho_out": rho_out},
+        "sha256": golden_io.state_digest(base, flags),
+        "mass": float(rho[m].sum()), "momentum": [float(ux[m].sum()), float(uy[m].sum()),
+                                                  float(uz[m].sum())],
+    }
+
+
 def main():
     O.build()
     arrays = {}
@@ -122,6 +175,11 @@ def main():
     case["solid_fraction"] = float((flags == 0).mean())
     cases.append(case)
     print(case["name"], case["sha256"][:16], case["n_fluid"])
+
+    for row in PRESSURE_CASES:
+        case = run_pressure_case(*row, arrays=arrays)
+        cases.append(case)
+        print(case["name"], case["sha256"][:16], case["n_fluid"])
 
     # the reference's own -V run: 16^3 box, x/y periodic, omega 1, F 1e-5,
     # 1000 steps from its (omega-scaled) equilibrium init, src/cli.c:84-99

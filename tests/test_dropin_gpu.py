@@ -19,7 +19,8 @@ pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CLI = os.path.join(ROOT, "lbm-bench_b200", "lbmbench-b200")
 CASES, _ = golden_io.load()
-STEP_CASES = [c for c in CASES if "verify" not in c]
+STEP_CASES = [c for c in CASES if "verify" not in c and "pressure" not in c]
+PRESSURE_CASES = [c for c in CASES if "pressure" in c]
 
 
 @pytest.mark.parametrize("kernel", ["cuda-pull-soa", "cuda-push-soa", "cuda-aa-soa"])

@@ -8,7 +8,8 @@ import golden_io
 import oracle as O
 
 CASES, _ = golden_io.load()
-STEP_CASES = [c for c in CASES if "verify" not in c]
+STEP_CASES = [c for c in CASES if "verify" not in c and "pressure" not in c]
+PRESSURE_CASES = [c for c in CASES if "pressure" in c]
 
 
 def test_velocity_set_tables():
@@ -105,3 +106,40 @@ def test_oracle_brinkman_zero_alpha_is_plain_step(oracle):
     a = oracle.run_brinkman(flags, (1, 0, 0), f0, 5, 1.1, 1 / 12, 1e-6, 0.0, por)
     b = oracle.run(flags, (1, 0, 0), f0, 5, 1.1, 1 / 12, 1e-6)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("case", PRESSURE_CASES, ids=[c["name"] for c in PRESSURE_CASES])
+def test_oracle_pressure_boundary_matches_golden(oracle, golden, case):
+    """Zou-He pressure boundary after every step (src/lbm.c:676-785): the
+    oracle gives the reference's pull/push state (golden digest)."""
+    _, arrays = golden
+    flags = golden_io.build_flags(case, arrays)
+    f0 = golden_io.initial_state(case, flags)
+    p = case["pressure"]
+    out = oracle.run_pressure(flags, case["periodic"], f0, case["steps"], case["omega"],
+                              case["lambda"], case["xforce"], bool(case["force_on"]),
+                              p["rho_in"], p["rho_out"])
+    assert golden_io.state_digest(out, flags) == case["sha256"]
+
+
+@pytest.mark.skipif(not O.ref_available("verify"), reason="oracle/_ref not built here")
+@pytest.mark.parametrize("seed", [1, 2, 3])
+@pytest.mark.parametrize("kernel", ["pull-soa", "push-soa"])
+def test_oracle_pressure_boundary_vs_live_reference(oracle, kernel, seed):
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = (int(v) for v in rng.integers(5, 13, size=3))
+    flags = np.ones((nz, ny, nx), dtype=np.int32)
+    flags[rng.uniform(size=flags.shape) < 0.2] = 0
+    flags[:, :, 0] = 2
+    flags[:, :, -1] = 4
+    flags[:, [0, -1], :] = 0
+    flags[[0, -1], :, :] = 0
+    f0 = O.perturbed_state(flags, seed, amp=2e-3)
+    steps = int(rng.integers(1, 9))
+    rho_in, rho_out = 1.0 + 0.01 * rng.uniform(), 1.0 - 0.01 * rng.uniform()
+    ref = O.Reference("verify")
+    out = ref.run_pressure(kernel, flags, (0, 0, 0), f0, steps, 1.2, 1e-6, rho_in, rho_out)
+    mine = oracle.run_pressure(flags, (0, 0, 0), f0, steps, 1.2, 1 / 12, 1e-6, True, rho_in,
+                               rho_out)
+    m = O.fluid_mask(flags)
+    assert np.array_equal(out[:, m], mine[:, m])

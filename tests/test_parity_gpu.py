@@ -17,7 +17,8 @@ import oracle as O
 pytestmark = pytest.mark.gpu
 
 CASES, _ = golden_io.load()
-STEP_CASES = [c for c in CASES if "verify" not in c]
+STEP_CASES = [c for c in CASES if "verify" not in c and "pressure" not in c]
+PRESSURE_CASES = [c for c in CASES if "pressure" in c]
 PATTERNS = ["pull", "push", "aa"]
 
 
@@ -256,3 +257,96 @@ def test_pipelined_kernels_full_size(porous256, monkeypatch, pattern, groups):
             outs[tma] = s.get_state()
     m = O.fluid_mask(flags)
     assert np.array_equal(outs["0"][:, m], outs["1"][:, m])
+
+
+# ---------------------------------------------------------------------------
+# Zou-He pressure boundary (src/lbm.c:676-785)
+# ---------------------------------------------------------------------------
+
+def _inlet_outlet(dims, solid, seed):
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = dims
+    flags = np.ones((nz, ny, nx), dtype=np.int32)
+    flags[rng.uniform(size=flags.shape) < solid] = 0
+    flags[:, :, 0] = 2
+    flags[:, :, -1] = 4
+    flags[:, [0, -1], :] = 0
+    flags[[0, -1], :, :] = 0
+    return flags
+
+
+def _pressure_run(flags, f0, steps, omega, lam, xforce, force_on, rho_in, rho_out, pattern,
+                  precision=L.F64):
+    with L.Solver(flags, (0, 0, 0), pattern, precision) as s:
+        s.set_params(omega, lam, xforce, force_on)
+        s.set_pressure_bc(rho_in, rho_out)
+        s.set_state(f0)
+        s.run(steps)
+        s.synchronize()
+        return s.get_state(), s.mass_momentum()[0]
+
+
+@pytest.mark.parametrize("pattern", PATTERNS)
+@pytest.mark.parametrize("case", PRESSURE_CASES, ids=[c["name"] for c in PRESSURE_CASES])
+def test_pressure_boundary_bit_identical_to_reference_fixtures(golden, case, pattern):
+    """The reference's pull and push kernels each followed by its Zou-He
+    pass give the golden digest; every pattern here must reproduce it (AA
+    too: the boundary follows each of its steps)."""
+    _, arrays = golden
+    flags = golden_io.build_flags(case, arrays)
+    f0 = golden_io.initial_state(case, flags)
+    p = case["pressure"]
+    out, _ = _pressure_run(flags, f0, case["steps"], case["omega"], case["lambda"],
+                           case["xforce"], bool(case["force_on"]), p["rho_in"], p["rho_out"],
+                           pattern)
+    assert golden_io.state_digest(out, flags) == case["sha256"]
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_pressure_boundary_bit_identical_to_oracle(oracle, seed):
+    rng = np.random.default_rng(200 + seed)
+    dims = tuple(int(v) for v in rng.integers(5, 16, size=3))
+    flags = _inlet_outlet(dims, 0.2, seed)
+    f0 = O.perturbed_state(flags, seed, amp=2e-3)
+    steps = int(rng.integers(1, 12))
+    rho_in, rho_out = 1.0 + 0.01 * rng.uniform(), 1.0 - 0.01 * rng.uniform()
+    ref = oracle.run_pressure(flags, (0, 0, 0), f0, steps, 1.3, 3 / 16, 1e-6, True, rho_in,
+                              rho_out)
+    m = O.fluid_mask(flags)
+    for pattern in PATTERNS:
+        out, _ = _pressure_run(flags, f0, steps, 1.3, 3 / 16, 1e-6, True, rho_in, rho_out,
+                               pattern)
+        assert np.array_equal(out[:, m], ref[:, m]), pattern
+
+
+@pytest.mark.parametrize("precision,tol", [(L.F32, 1e-5), (L.F16, 2e-3)])
+def test_pressure_boundary_reduced_precision(precision, tol):
+    """A pressure-driven channel (64 cells long, rho 1.01 -> 0.99) with the
+    boundary in FP32/FP16 storage tracks FP64, and the flow goes from the
+    high-pressure inlet to the outlet."""
+    flags = _inlet_outlet((64, 18, 20), 0.0, 1)
+    f0 = L.perturbed_equilibrium(flags, seed=3, amplitude=1e-4)
+    a, ta = _pressure_run(flags, f0, 400, 1.25, 3 / 16, 0.0, False, 1.01, 0.99, "aa")
+    b, tb = _pressure_run(flags, f0, 400, 1.25, 3 / 16, 0.0, False, 1.01, 0.99, "aa", precision)
+    r2, x2, _, _ = O.moments(a, flags)
+    r3, x3, _, _ = O.moments(b, flags)
+    m = O.fluid_mask(flags)
+    assert ta[1] > 0.0  # x momentum from inlet to outlet
+    assert np.linalg.norm(x3[m] - x2[m]) <= tol * np.linalg.norm(x2[m])
+    # density drops from inlet to outlet
+    assert r2[1][m[1]].mean() > r2[-2][m[-2]].mean()
+
+
+def test_pressure_boundary_argument_errors():
+    flags, per, _ = L.geometry("channel", (10, 8, 8))
+    with L.Solver(flags, per, "aa") as s:
+        with pytest.raises(L.LbmError):
+            s.set_pressure_bc(1.01, 0.99)  # no inlet/outlet cells
+        s.set_pressure_bc(1.0, 1.0, on=False)
+    flags = _inlet_outlet((10, 8, 8), 0.0, 2)
+    with L.Solver(flags, (0, 0, 0), "aa") as s:
+        with pytest.raises(L.LbmError):
+            s.set_pressure_bc(-1.0, 0.99)
+        s.set_pressure_bc(1.01, 0.99)
+        s.run(2)
+        s.synchronize()
