@@ -9,11 +9,10 @@
 //     missing half from the neighbouring lane with one warp shuffle; only
 //     lane 0 (s = -1) or lane 31 (s = +1) loads a single element from the
 //     next 64-cell segment of the row (wrapping around a periodic z);
-//   * a scatter shifted by s builds the aligned target pair from its own
-//     value and the neighbouring lane's, and stores it as one pair; lane 31
-//     (s = +1) or lane 0 (s = -1) stores its one leftover element.
-// There is no per-lane address choice anywhere except the bounce-back
-// redirects, which are predicated single-element accesses. Requires
+//   * a scatter shifted by s stores each fluid cell's own element (two
+//     16-bit stores per lane; realigning them into pairs with shuffles,
+//     which needs per-lane ownership of the target pairs, measured slower).
+// The bounce-back redirects are predicated single-element accesses. Requires
 // nz % 64 == 0 and blockDim.x == 32; other extents use step_kernel_x2.
 // Bounce-back, force and the Brinkman term follow step_kernel
 // (lbm_step.cuh): a population that bounced off the wall x - c_d is read
@@ -51,13 +50,6 @@ __global__ void __launch_bounds__(kStepThreads, (PairOccupancy<ST, KIND, true>::
   // directions in which any cell of the warp has a wall link (uniform)
   const uint32_t wlinks = __reduce_or_sync(kFull, (m0 | m1) & 0x7FFFFu);
   const bool links = wlinks != 0u;
-  // which halves of the aligned target pairs a lane owns in a z-shifted
-  // scatter (the same for every direction of one shift sign): for +1 the
-  // pair (z, z+1) takes cells (z-1, z), for -1 cells (z+1, z+2); a wall cell
-  // writes nothing, and the half fed from the next segment is written there
-  const unsigned f1bits = __ballot_sync(kFull, fluid1), f0bits = __ballot_sync(kFull, fluid0);
-  const bool up_x = lane > 0 && ((f1bits >> (lane - 1)) & 1u), up_y = fluid0;
-  const bool dn_x = fluid1, dn_y = lane < 31 && ((f0bits >> (lane + 1)) & 1u);
 
   // x/y parts of the neighbour offsets (uniform across the warp); the z
   // shift is handled by shuffles and the two edge lanes
@@ -170,9 +162,9 @@ __global__ void __launch_bounds__(kStepThreads, (PairOccupancy<ST, KIND, true>::
       *reinterpret_cast<P *>(dst + d * PL + cell) = PT::enc(v);
       continue;
     }
-    // push / AA odd: every population to (d, x + c_d); the aligned pair
-    // (z, z+1) of the target row is written whole where this lane owns both
-    // halves, otherwise half by half (independent predicated stores)
+    // push / AA odd: every population to (d, x + c_d); unshifted in z the
+    // aligned pair (z, z+1) of the target row is written whole when both
+    // cells are fluid, otherwise half by half
     const float2 v = FORCE ? add2(out[d], f2(a.c.force[d])) : out[d];
     S *base = dst + d * PL + (uint32_t)(cell + row(d));
     float2 t;
@@ -181,18 +173,15 @@ __global__ void __launch_bounds__(kStepThreads, (PairOccupancy<ST, KIND, true>::
       t = v;
       tx = fluid0;
       ty = fluid1;
-    } else if (cz(d) > 0) { // targets z + 1, z + 2
-      t = make_float2(__shfl_up_sync(kFull, v.y, 1), v.x);
-      tx = up_x;
-      ty = up_y;
-      if (lane == 31 && fluid1) // cell z+1 -> z+2, first element of the next segment
-        base[hi] = PT::enc1(v.y);
-    } else { // targets z - 1, z
-      t = make_float2(v.y, __shfl_down_sync(kFull, v.x, 1));
-      tx = dn_x;
-      ty = dn_y;
-      if (lane == 0 && fluid0) // cell z -> z-1, last element of the previous segment
-        base[lo] = PT::enc1(v.x);
+    } else {
+      // shifted in z: each fluid cell stores its own element, at offset lo
+      // (z -> z - 1) or hi (z + 1 -> z + 2), which wrap at the row ends
+      if (fluid0)
+        base[cz(d) < 0 ? lo : 1] = PT::enc1(v.x);
+      if (fluid1)
+        base[cz(d) < 0 ? 0 : hi] = PT::enc1(v.y);
+      t = v;
+      tx = ty = false;
     }
     if (tx && ty)
       *reinterpret_cast<P *>(base) = PT::enc(t);
