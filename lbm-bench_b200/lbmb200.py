@@ -411,54 +411,73 @@ class LatticeDesc(ctypes.Structure):
                 ("Name", ctypes.c_char_p)]
 
 
-class CaseData(ctypes.Structure):
-    """CaseDataType of the reference's double build (src/lbm.h:68-75)."""
-    _fields_ = [("Omega", ctypes.c_double), ("RhoIn", ctypes.c_double),
-                ("RhoOut", ctypes.c_double), ("XForce", ctypes.c_double),
-                ("MaxIterations", ctypes.c_int), ("StatisticsModulus", ctypes.c_int)]
+def _dropin_types(pdf):
+    """ctypes mirrors of CaseDataType, KernelDataType and KernelFunctionsType
+    (src/lbm.h:68-106) for PdfType = pdf (c_double, or c_float in a
+    PRECISION_SP build)."""
+
+    class CaseData(ctypes.Structure):
+        _fields_ = [("Omega", pdf), ("RhoIn", pdf), ("RhoOut", pdf), ("XForce", pdf),
+                    ("MaxIterations", ctypes.c_int), ("StatisticsModulus", ctypes.c_int)]
+
+    class KernelData(ctypes.Structure):
+        pass
+
+    node_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(KernelData), ctypes.c_int, ctypes.c_int,
+                               ctypes.c_int, ctypes.POINTER(pdf))
+    bcget_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(KernelData), ctypes.c_int, ctypes.c_int,
+                                ctypes.c_int, ctypes.c_int, ctypes.POINTER(pdf))
+    bcset_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(KernelData), ctypes.c_int, ctypes.c_int,
+                                ctypes.c_int, ctypes.c_int, pdf)
+    kernel_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(LatticeDesc), ctypes.POINTER(KernelData),
+                                 ctypes.POINTER(CaseData))
+    KernelData._fields_ = [
+        ("Pdfs", ctypes.POINTER(pdf) * 2), ("PdfsActive", ctypes.POINTER(pdf)),
+        ("Dims", ctypes.c_int * 3), ("GlobalDims", ctypes.c_int * 3), ("Offsets", ctypes.c_int * 3),
+        ("BounceBackPdfsSrc", ctypes.POINTER(ctypes.c_int)),
+        ("BounceBackPdfsDst", ctypes.POINTER(ctypes.c_int)), ("nBounceBackPdfs", ctypes.c_int),
+        ("Blk", ctypes.c_int * 3), ("Iteration", ctypes.c_int), ("LoopBalance", ctypes.c_double),
+        ("Duration", ctypes.c_double), ("GetNode", node_fn), ("SetNode", node_fn),
+        ("BoundaryConditionsGetPdf", bcget_fn), ("BoundaryConditionsSetPdf", bcset_fn),
+        ("Kernel", kernel_fn)]
+    init_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(LatticeDesc),
+                               ctypes.POINTER(ctypes.POINTER(KernelData)), ctypes.POINTER(CaseData))
+    deinit_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(LatticeDesc),
+                                 ctypes.POINTER(ctypes.POINTER(KernelData)))
+
+    class KernelFunctions(ctypes.Structure):
+        _fields_ = [("Name", ctypes.c_char_p), ("Init", init_fn), ("Deinit", deinit_fn)]
+
+    return CaseData, KernelData, KernelFunctions
 
 
-class KernelData(ctypes.Structure):
-    pass
+# the reference's default (double) build
+CaseData, KernelData, KernelFunctions = _dropin_types(ctypes.c_double)
+CaseDataSP, KernelDataSP, KernelFunctionsSP = _dropin_types(ctypes.c_float)
+LIB_PATH_SP = os.path.join(HERE, "liblbmb200_sp.so")
+_lib_sp = None
 
 
-_node_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(KernelData), ctypes.c_int, ctypes.c_int,
-                            ctypes.c_int, ctypes.POINTER(ctypes.c_double))
-_bcget_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(KernelData), ctypes.c_int, ctypes.c_int,
-                             ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double))
-_bcset_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(KernelData), ctypes.c_int, ctypes.c_int,
-                             ctypes.c_int, ctypes.c_int, ctypes.c_double)
-_kernel_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(LatticeDesc), ctypes.POINTER(KernelData),
-                              ctypes.POINTER(CaseData))
-KernelData._fields_ = [
-    ("Pdfs", ctypes.POINTER(ctypes.c_double) * 2), ("PdfsActive", ctypes.POINTER(ctypes.c_double)),
-    ("Dims", ctypes.c_int * 3), ("GlobalDims", ctypes.c_int * 3), ("Offsets", ctypes.c_int * 3),
-    ("BounceBackPdfsSrc", ctypes.POINTER(ctypes.c_int)),
-    ("BounceBackPdfsDst", ctypes.POINTER(ctypes.c_int)), ("nBounceBackPdfs", ctypes.c_int),
-    ("Blk", ctypes.c_int * 3), ("Iteration", ctypes.c_int), ("LoopBalance", ctypes.c_double),
-    ("Duration", ctypes.c_double), ("GetNode", _node_fn), ("SetNode", _node_fn),
-    ("BoundaryConditionsGetPdf", _bcget_fn), ("BoundaryConditionsSetPdf", _bcset_fn),
-    ("Kernel", _kernel_fn)]
-
-_init_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(LatticeDesc),
-                            ctypes.POINTER(ctypes.POINTER(KernelData)), ctypes.POINTER(CaseData))
-_deinit_fn = ctypes.CFUNCTYPE(None, ctypes.POINTER(LatticeDesc),
-                              ctypes.POINTER(ctypes.POINTER(KernelData)))
+def lib_sp():
+    """liblbmb200_sp.so: the drop-in kernels for a PRECISION_SP build."""
+    global _lib_sp
+    if _lib_sp is None:
+        if not os.path.exists(LIB_PATH_SP):
+            raise OSError(f"{LIB_PATH_SP} not built (make -C lbm-bench_b200)")
+        _lib_sp = ctypes.CDLL(LIB_PATH_SP)
+    return _lib_sp
 
 
-class KernelFunctions(ctypes.Structure):
-    _fields_ = [("Name", ctypes.c_char_p), ("Init", _init_fn), ("Deinit", _deinit_fn)]
-
-
-def _registry():
-    L = lib()
+def _registry(sp=False):
+    L = lib_sp() if sp else lib()
+    kf = KernelFunctionsSP if sp else KernelFunctions
     n = ctypes.c_int.in_dll(L, "LBM_B200_N_KERNELS").value
-    return (KernelFunctions * n).in_dll(L, "LbmB200Kernels")
+    return (kf * n).in_dll(L, "LbmB200Kernels")
 
 
-def dropin_kernels():
+def dropin_kernels(sp=False):
     """Names in the library's registry (LbmB200Kernels)."""
-    return [k.Name.decode() for k in _registry()]
+    return [k.Name.decode() for k in _registry(sp)]
 
 
 class DropIn:
@@ -467,9 +486,12 @@ class DropIn:
     Kernel, GetNode, Deinit."""
 
     def __init__(self, name, flags, periodic, omega=1.0, xforce=1e-5, iterations=10,
-                 force_on=None, lam=None):
-        L = lib()
-        self.kf = next((k for k in _registry() if k.Name.decode() == name), None)
+                 force_on=None, lam=None, sp=False):
+        L = lib_sp() if sp else lib()
+        self.sp = sp
+        pdf = ctypes.c_float if sp else ctypes.c_double
+        case_t = CaseDataSP if sp else CaseData
+        self.kf = next((k for k in _registry(sp) if k.Name.decode() == name), None)
         if self.kf is None:
             raise KeyError(name)
         L.lbmB200SetBodyForce.argtypes = [ctypes.c_int]
@@ -487,10 +509,10 @@ class DropIn:
         self.ld.nObst = self.ld.nCells - self.ld.nFluid
         self.ld.PeriodicX, self.ld.PeriodicY, self.ld.PeriodicZ = (int(p) for p in periodic)
         self.ld.Name = b"python"
-        self.cd = CaseData(omega, 1.0, 1.0, xforce, iterations, 100)
-        self.kd = ctypes.POINTER(KernelData)()
+        self.cd = case_t(omega, 1.0, 1.0, xforce, iterations, 100)
+        self.kd = ctypes.POINTER(KernelDataSP if sp else KernelData)()
         self.kf.Init(ctypes.byref(self.ld), ctypes.byref(self.kd), ctypes.byref(self.cd))
-        self._buf = (ctypes.c_double * Q)()
+        self._buf = (pdf * Q)()
 
     @property
     def data(self) -> KernelData:

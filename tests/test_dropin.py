@@ -40,13 +40,21 @@ def test_dropin_struct_layout_equals_reference_lbm_h(tmp_path, sp):
     assert ours == theirs
 
 
-def test_ctypes_mirror_matches_the_c_layout(tmp_path):
-    out = dict(line.rsplit(" ", 1) for line in _probe(tmp_path).splitlines())
-    assert int(out["sizeof KernelDataType"]) == ctypes.sizeof(L.KernelData)
+@pytest.mark.parametrize("sp", [False, True])
+def test_ctypes_mirror_matches_the_c_layout(tmp_path, sp):
+    out = dict(line.rsplit(" ", 1)
+               for line in _probe(tmp_path, *(["-DPRECISION_SP"] if sp else [])).splitlines())
+    kd, cd = (L.KernelDataSP, L.CaseDataSP) if sp else (L.KernelData, L.CaseData)
+    assert int(out["sizeof PdfType"]) == (4 if sp else 8)
+    assert int(out["sizeof KernelDataType"]) == ctypes.sizeof(kd)
     assert int(out["sizeof LatticeDescType"]) == ctypes.sizeof(L.LatticeDesc)
-    assert int(out["sizeof CaseDataType"]) == ctypes.sizeof(L.CaseData)
-    assert int(out["KernelDataType.Kernel"]) == L.KernelData.Kernel.offset
-    assert int(out["KernelDataType.Duration"]) == L.KernelData.Duration.offset
+    assert int(out["sizeof CaseDataType"]) == ctypes.sizeof(cd)
+    assert int(out["KernelDataType.Kernel"]) == kd.Kernel.offset
+    assert int(out["KernelDataType.Duration"]) == kd.Duration.offset
+
+
+def test_single_precision_registry():
+    assert L.dropin_kernels(sp=True) == L.dropin_kernels()
 
 
 def test_registry_names():

@@ -82,6 +82,29 @@ def test_dropin_reduced_precision_tracks_fp64():
         assert np.abs(out[:, m] - ref[:, m]).max() < tol, name
 
 
+@pytest.mark.parametrize("kernel", ["cuda-pull-soa", "cuda-push-soa", "cuda-aa-soa"])
+def test_dropin_single_precision_build(kernel):
+    """liblbmb200_sp.so, for a reference built with PRECISION_SP (PdfType
+    float, src/lbm.h:48-52): float host lattices and CaseData, FP32 device
+    storage, results within FP32 rounding of the FP64 oracle."""
+    flags, per, _ = L.geometry("blocks-4", (22, 18, 20))
+    f0 = L.perturbed_equilibrium(flags, seed=13, amplitude=1e-3)
+    m = O.fluid_mask(flags)
+    ref = O.Oracle().run(flags, per, f0, 8, 1.4, 1 / 12, 1e-5, True)
+    with L.DropIn(kernel, flags, per, omega=1.4, iterations=8, force_on=True, sp=True) as k:
+        assert ctypes.sizeof(k.data.Pdfs[0]._type_) == 4
+        assert k.data.LoopBalance == 2 * 19 * 4
+        k.set_state(f0)
+        k.run()
+        # pull / push end in Pdfs[0] after an even number of swaps; AA in its one lattice
+        addr = lambda p: ctypes.cast(p, ctypes.c_void_p).value  # noqa: E731
+        assert addr(k.data.PdfsActive) == addr(k.data.Pdfs[0])
+        out = k.get_state()
+        assert out.dtype == np.float64
+    err = np.abs(out[:, m] - ref[:, m]).max()
+    assert 0 < err < 1e-6
+
+
 @pytest.mark.parametrize("kernel", L.dropin_kernels() if os.path.exists(L.LIB_PATH) else [])
 def test_cli_verification_run_succeeds(kernel):
     """The reference's test.sh runs `lbmbench -V -k K` for every kernel `-l`
