@@ -108,6 +108,10 @@ int lbm_get_state(lbm_solver *s, double *f);
 #define LBM_REF_NATURAL 0
 #define LBM_REF_PULL 1
 #define LBM_REF_AA_EVEN 2
+/* OR into ref_orientation: the array is in the reference's AoS order
+ * (indexAoS, src/lbm.h:118-121: the 19 values of a padded cell are
+ * contiguous), as its pull-aos / push-aos kernels keep it. */
+#define LBM_REF_AOS 16
 
 /* Uploads / downloads the state from / to an array in the reference's
  * padded layout and the given orientation; elem_size 8 (PdfType double) or

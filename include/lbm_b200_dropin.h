@@ -10,7 +10,8 @@
  * to GKernels[] and links liblbmb200.
  *
  * The kernel data the Init functions return keeps the reference's host
- * arrays (Pdfs[0..1] in the padded indexSoA layout, page-locked) and
+ * arrays (Pdfs[0..1] in the padded indexSoA layout, or indexAoS for the
+ * AoS names, page-locked) and
  * accessors; Kernel copies PdfsActive to the GPU, runs cd->MaxIterations
  * steps there (AA: rounded up to an even count, as src/kernel_aa_soa.c:36
  * does), times only the step loop into kd->Duration, and copies the result
@@ -100,6 +101,17 @@ typedef struct KernelFunctions {
 void kernelInitCudaPullSoA(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
 void kernelInitCudaPushSoA(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
 void kernelInitCudaAaSoA(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
+/* The reference's layout variants (kernelInitPullAoS / kernelInitPushAoS /
+ * kernelInitBlkPushSoA / kernelInitBlkPullSoA, src/lbm.c:608-651): the AoS
+ * names keep Pdfs[] and the accessors in indexAoS order (src/lbm.h:118-121),
+ * the blk names set kd->Blk to 8^3 and print the reference's blocking line.
+ * On the GPU all of them run the SoA kernels of their pattern (an AoS device
+ * layout would split every warp's load of one population over 19x as many
+ * sectors); results equal the SoA names' bit for bit. */
+void kernelInitCudaPullAoS(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
+void kernelInitCudaPushAoS(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
+void kernelInitCudaBlkPushSoA(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
+void kernelInitCudaBlkPullSoA(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
 void kernelInitCudaPullSoAFp32(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
 void kernelInitCudaPushSoAFp32(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);
 void kernelInitCudaAaSoAFp32(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd);

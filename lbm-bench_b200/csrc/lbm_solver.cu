@@ -961,9 +961,114 @@ __global__ void unpack_ref_kernel(Grid g, UserBox u, int p, int ref_orient, int 
   plane[ref_index(u.nx + 2, u.ny + 2, u.nz + 2, ref_orient, d, x, y, z)] = (H)v;
 }
 
+// The same transfer for the reference's AoS array (indexAoS,
+// src/lbm.h:118-121): padded x-planes [a0, a0 + gridDim.z) of it sit in
+// `chunk`, and each thread takes the 19 contiguous slots of one padded cell.
+// A slot maps back to the fluid cell whose population it holds (the inverse
+// of ref_index); on download slots that hold none are written as 0.
+template <class ST, typename H, bool UP>
+__global__ void aos_ref_kernel(Grid g, UserBox u, int a0, int ref_orient, int orient,
+    H *__restrict__ chunk, typename ST::S *state, const uint32_t *__restrict__ mask, float scale)
+{
+  using V = typename ST::V;
+  const int rz = u.nz + 2, ry = u.ny + 2;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y * blockDim.y + threadIdx.y;
+  const int a = a0 + (int)blockIdx.z;
+  if (c >= rz || b >= ry)
+    return;
+  H *slots = chunk + (((long long)blockIdx.z * ry + b) * rz + c) * Q;
+#pragma unroll 1
+  for (int p = 0; p < Q; ++p) {
+    const int d = (ref_orient == LBM_REF_AA_EVEN) ? inv(p) : p;
+    int x = a - 1, y = b - 1, z = c - 1;
+    if (ref_orient != LBM_REF_NATURAL) {
+      x += cx(d);
+      y += cy(d);
+      z += cz(d);
+    }
+    bool own = x >= 0 && x < u.nx && y >= 0 && y < u.ny && z >= 0 && z < u.nz;
+    uint32_t cell = 0, m = kSolidBit;
+    if (own) {
+      cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
+      m = mask[cell];
+      own = !(m & kSolidBit);
+    }
+    if (!own) {
+      if (!UP)
+        slots[p] = (H)0;
+      continue;
+    }
+    const Offs nb = make_offs(g, x + u.ox, y + u.oy, z + u.oz);
+    int sp;
+    uint32_t sc;
+    state_slot(orient, d, m, cell, nb, sp, sc);
+    const int wc = wclass(d);
+    const double w = wc == 0 ? 1.0 / 3.0 : wc == 1 ? 1.0 / 18.0 : 1.0 / 36.0;
+    if (UP) {
+      double v = (double)slots[p];
+      if (ST::kShifted)
+        v -= w;
+      ST::store(state + (long long)sp * g.plane + sc, (V)v, (V)scale);
+    } else {
+      double v = (double)ST::load(state + (long long)sp * g.plane + sc, d, (V)scale);
+      if (ST::kShifted)
+        v += w;
+      slots[p] = (H)v;
+    }
+  }
+}
+
+template <class ST, typename H>
+static int ref_transfer_aos(lbm_solver *s, void *host, int ref_orient, bool upload)
+{
+  const int ra = s->nx + 2, ry = s->ny + 2, rz = s->nz + 2;
+  const size_t xplane = (size_t)ry * rz * Q; // values of one padded x-plane
+  // as many x-planes per chunk as fit the staging of one SoA direction plane
+  const size_t gpl = (size_t)ra * ry * rz;
+  const int per = (int)(gpl / xplane) > 0 ? (int)(gpl / xplane) : 1;
+  const size_t bytes = (size_t)per * xplane * sizeof(H);
+  if (s->pstaging_bytes < bytes) {
+    cudaFree(s->pstaging);
+    s->pstaging = NULL;
+    s->pstaging_bytes = 0;
+    int rc = dev_alloc(s, &s->pstaging, bytes, "the padded transfer plane");
+    if (rc)
+      return rc;
+    s->pstaging_bytes = bytes;
+  }
+  const int o = orientation(s);
+  const float sc = (float)(s->precision == LBM_F16 ? s->fp16_scale : 1.0);
+  using Sx = typename ST::S;
+  H *hp = (H *)host;
+  H *dp = (H *)s->pstaging;
+  const dim3 block(32, 8, 1);
+  for (int a0 = 0; a0 < ra; a0 += per) {
+    const int n = ra - a0 < per ? ra - a0 : per;
+    const dim3 grid((rz + 31) / 32, (ry + 7) / 8, n);
+    const size_t nbytes = (size_t)n * xplane * sizeof(H);
+    H *hc = hp + (size_t)a0 * xplane;
+    if (upload) {
+      CUDA_TRY(cudaMemcpyAsync(dp, hc, nbytes, cudaMemcpyHostToDevice, s->stream));
+      aos_ref_kernel<ST, H, true><<<grid, block, 0, s->stream>>>(s->g, s->ub, a0, ref_orient, o,
+          dp, (Sx *)state_ptr(s), s->mask, sc);
+      CUDA_TRY(cudaGetLastError());
+    } else {
+      aos_ref_kernel<ST, H, false><<<grid, block, 0, s->stream>>>(s->g, s->ub, a0, ref_orient,
+          o, dp, (Sx *)state_ptr(s), s->mask, 1.0f / sc);
+      CUDA_TRY(cudaGetLastError());
+      CUDA_TRY(cudaMemcpyAsync(hc, dp, nbytes, cudaMemcpyDeviceToHost, s->stream));
+    }
+  }
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return LBM_OK;
+}
+
 template <class ST, typename H>
 static int ref_transfer(lbm_solver *s, void *host, int ref_orient, bool upload)
 {
+  if (ref_orient & LBM_REF_AOS)
+    return ref_transfer_aos<ST, H>(s, host, ref_orient & ~LBM_REF_AOS, upload);
   const size_t gpl = (size_t)(s->nx + 2) * (s->ny + 2) * (s->nz + 2);
   const size_t bytes = gpl * sizeof(H);
   if (s->pstaging_bytes < bytes) {
@@ -1003,8 +1108,9 @@ static int ref_transfer(lbm_solver *s, void *host, int ref_orient, bool upload)
 
 static int ref_dispatch(lbm_solver *s, void *host, int elem_size, int ref_orient, bool upload)
 {
-  if (!s || !host || (elem_size != 8 && elem_size != 4) || ref_orient < LBM_REF_NATURAL ||
-      ref_orient > LBM_REF_AA_EVEN)
+  const int o = ref_orient & ~LBM_REF_AOS;
+  if (!s || !host || (elem_size != 8 && elem_size != 4) || o < LBM_REF_NATURAL ||
+      o > LBM_REF_AA_EVEN)
     return fail(LBM_ERR_ARG, "padded transfer: bad arguments");
   CUDA_TRY(cudaSetDevice(s->device));
   if (elem_size == 8) {

@@ -21,6 +21,7 @@ typedef struct {
   KernelDataType kd;
   lbm_solver *solver;
   int pattern;
+  int aos; /* host lattices in indexAoS order (pull-aos / push-aos) */
   size_t pdf_bytes;
   int pinned[2];
 } CudaKernelData;
@@ -49,6 +50,12 @@ static void die(const char *what)
 static long long soa(const int *g, int x, int y, int z, int d)
 {
   return (((long long)d * g[0] + x) * g[1] + y) * g[2] + z;
+}
+
+/* indexAoS of the reference (src/lbm.h:118-121) in 64-bit */
+static long long aos(const int *g, int x, int y, int z, int d)
+{
+  return (((long long)x * g[1] + y) * g[2] + z) * Q + d;
 }
 
 /* Node accessors with the reference's slot rules (src/lbm.c:193-294):
@@ -91,9 +98,23 @@ static long long slot_aa(KernelDataType *kd, int x, int y, int z, int d)
     kd->PdfsActive[SLOT(kd, x, y, z, d)] = pdf;                                              \
   }
 
+/* the AoS kernels' accessors: the same slots in indexAoS order
+ * (src/lbm.c:227-258) */
+static long long slot_push_aos(KernelDataType *kd, int x, int y, int z, int d)
+{
+  return aos(kd->GlobalDims, x + kd->Offsets[0], y + kd->Offsets[1], z + kd->Offsets[2], d);
+}
+static long long slot_pull_aos(KernelDataType *kd, int x, int y, int z, int d)
+{
+  return aos(kd->GlobalDims, x + kd->Offsets[0] - CX[d], y + kd->Offsets[1] - CY[d],
+      z + kd->Offsets[2] - CZ[d], d);
+}
+
 ACCESSORS(Push, slot_push)
 ACCESSORS(Pull, slot_pull)
 ACCESSORS(Aa, slot_aa)
+ACCESSORS(PushAos, slot_push_aos)
+ACCESSORS(PullAos, slot_pull_aos)
 
 /* Number of entries the reference's bounce-back list would hold for this
  * lattice (src/lbm.c:465-494): for every fluid cell and direction, the
@@ -136,7 +157,8 @@ static void cudaKernel(LatticeDescType *ld, KernelDataType *kd, CaseDataType *cd
 
   /* like the reference, every run starts from Pdfs[0] in the pattern's
    * natural orientation (src/kernel_pull_soa.c:35, src/kernel_aa_soa.c:29) */
-  const int ref_o = (ck->pattern == LBM_PULL) ? LBM_REF_PULL : LBM_REF_NATURAL;
+  const int ref_o = ((ck->pattern == LBM_PULL) ? LBM_REF_PULL : LBM_REF_NATURAL) |
+      (ck->aos ? LBM_REF_AOS : 0);
   if (lbm_set_state_padded(ck->solver, kd->Pdfs[0], (int)sizeof(PdfType), ref_o) != LBM_OK)
     die("cuda kernel upload");
   double ms = 0.0;
@@ -155,8 +177,14 @@ static void cudaKernel(LatticeDescType *ld, KernelDataType *kd, CaseDataType *cd
     kd->Iteration = steps - 1;
 }
 
+/* Host layouts of the registered kernels: SoA, the AoS order of the
+ * reference's pull-aos / push-aos, or SoA with the 8^3 blocking the
+ * reference's blk-*-soa kernels record in kd->Blk (src/lbm.c:629-651). The
+ * device state is SoA in every case. */
+enum { HOST_SOA, HOST_AOS, HOST_BLK };
+
 static void initCuda(LatticeDescType *ld, KernelDataType **kdp, int pattern, int precision,
-    const char *name)
+    const char *name, int host_layout)
 {
   CudaKernelData *ck = (CudaKernelData *)calloc(1, sizeof(CudaKernelData));
   if (!ck) {
@@ -165,11 +193,12 @@ static void initCuda(LatticeDescType *ld, KernelDataType **kdp, int pattern, int
   }
   KernelDataType *kd = &ck->kd;
   ck->pattern        = pattern;
+  ck->aos            = host_layout == HOST_AOS;
   for (int a = 0; a < 3; ++a) {
     kd->Dims[a]       = ld->Dims[a];
     kd->GlobalDims[a] = ld->Dims[a] + 2;
     kd->Offsets[a]    = 1;
-    kd->Blk[a]        = kd->GlobalDims[a];
+    kd->Blk[a]        = host_layout == HOST_BLK ? 8 : kd->GlobalDims[a];
   }
   kd->Iteration = -1;
   const long long cells =
@@ -192,7 +221,17 @@ static void initCuda(LatticeDescType *ld, KernelDataType **kdp, int pattern, int
   kd->BounceBackPdfsDst = NULL;
   kd->nBounceBackPdfs   = count_bounce_back(ld, pattern);
   kd->LoopBalance       = 2.0 * Q * sizeof(PdfType);
-  if (pattern == LBM_PUSH) {
+  if (pattern == LBM_PUSH && ck->aos) {
+    kd->GetNode                  = getNodePushAos;
+    kd->SetNode                  = setNodePushAos;
+    kd->BoundaryConditionsGetPdf = bcGetPushAos;
+    kd->BoundaryConditionsSetPdf = bcSetPushAos;
+  } else if (pattern == LBM_PULL && ck->aos) {
+    kd->GetNode                  = getNodePullAos;
+    kd->SetNode                  = setNodePullAos;
+    kd->BoundaryConditionsGetPdf = bcGetPullAos;
+    kd->BoundaryConditionsSetPdf = bcSetPullAos;
+  } else if (pattern == LBM_PUSH) {
     kd->GetNode                  = getNodePush;
     kd->SetNode                  = setNodePush;
     kd->BoundaryConditionsGetPdf = bcGetPush;
@@ -216,6 +255,8 @@ static void initCuda(LatticeDescType *ld, KernelDataType **kdp, int pattern, int
       cells, nbuf * ck->pdf_bytes / 1048576.0, nbuf == 1 ? "single lattice" : "both lattices",
       lbm_device_bytes(ck->solver) / 1048576.0);
   printf("# bounce-back PDFs: %d\n", kd->nBounceBackPdfs);
+  if (host_layout == HOST_BLK)
+    printf("# blocking x: %3d y: %3d z: %3d\n", kd->Blk[0], kd->Blk[1], kd->Blk[2]);
   *kdp = kd;
 }
 
@@ -228,47 +269,67 @@ static void initCuda(LatticeDescType *ld, KernelDataType **kdp, int pattern, int
 void kernelInitCudaPullSoA(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd)
 {
   (void)cd;
-  initCuda(ld, kd, LBM_PULL, NATIVE_PRECISION, "cuda-pull-soa");
+  initCuda(ld, kd, LBM_PULL, NATIVE_PRECISION, "cuda-pull-soa", HOST_SOA);
 }
 void kernelInitCudaPushSoA(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd)
 {
   (void)cd;
-  initCuda(ld, kd, LBM_PUSH, NATIVE_PRECISION, "cuda-push-soa");
+  initCuda(ld, kd, LBM_PUSH, NATIVE_PRECISION, "cuda-push-soa", HOST_SOA);
 }
 void kernelInitCudaAaSoA(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd)
 {
   (void)cd;
-  initCuda(ld, kd, LBM_AA, NATIVE_PRECISION, "cuda-aa-soa");
+  initCuda(ld, kd, LBM_AA, NATIVE_PRECISION, "cuda-aa-soa", HOST_SOA);
+}
+void kernelInitCudaPullAoS(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd)
+{
+  (void)cd;
+  initCuda(ld, kd, LBM_PULL, NATIVE_PRECISION, "cuda-pull-aos", HOST_AOS);
+}
+void kernelInitCudaPushAoS(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd)
+{
+  (void)cd;
+  initCuda(ld, kd, LBM_PUSH, NATIVE_PRECISION, "cuda-push-aos", HOST_AOS);
+}
+void kernelInitCudaBlkPushSoA(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd)
+{
+  (void)cd;
+  initCuda(ld, kd, LBM_PUSH, NATIVE_PRECISION, "cuda-blk-push-soa", HOST_BLK);
+}
+void kernelInitCudaBlkPullSoA(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd)
+{
+  (void)cd;
+  initCuda(ld, kd, LBM_PULL, NATIVE_PRECISION, "cuda-blk-pull-soa", HOST_BLK);
 }
 void kernelInitCudaPullSoAFp32(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd)
 {
   (void)cd;
-  initCuda(ld, kd, LBM_PULL, LBM_F32, "cuda-pull-soa-fp32");
+  initCuda(ld, kd, LBM_PULL, LBM_F32, "cuda-pull-soa-fp32", HOST_SOA);
 }
 void kernelInitCudaPushSoAFp32(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd)
 {
   (void)cd;
-  initCuda(ld, kd, LBM_PUSH, LBM_F32, "cuda-push-soa-fp32");
+  initCuda(ld, kd, LBM_PUSH, LBM_F32, "cuda-push-soa-fp32", HOST_SOA);
 }
 void kernelInitCudaAaSoAFp32(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd)
 {
   (void)cd;
-  initCuda(ld, kd, LBM_AA, LBM_F32, "cuda-aa-soa-fp32");
+  initCuda(ld, kd, LBM_AA, LBM_F32, "cuda-aa-soa-fp32", HOST_SOA);
 }
 void kernelInitCudaPullSoAFp16(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd)
 {
   (void)cd;
-  initCuda(ld, kd, LBM_PULL, LBM_F16, "cuda-pull-soa-fp16");
+  initCuda(ld, kd, LBM_PULL, LBM_F16, "cuda-pull-soa-fp16", HOST_SOA);
 }
 void kernelInitCudaPushSoAFp16(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd)
 {
   (void)cd;
-  initCuda(ld, kd, LBM_PUSH, LBM_F16, "cuda-push-soa-fp16");
+  initCuda(ld, kd, LBM_PUSH, LBM_F16, "cuda-push-soa-fp16", HOST_SOA);
 }
 void kernelInitCudaAaSoAFp16(LatticeDescType *ld, KernelDataType **kd, CaseDataType *cd)
 {
   (void)cd;
-  initCuda(ld, kd, LBM_AA, LBM_F16, "cuda-aa-soa-fp16");
+  initCuda(ld, kd, LBM_AA, LBM_F16, "cuda-aa-soa-fp16", HOST_SOA);
 }
 
 void kernelDeinitCuda(LatticeDescType *ld, KernelDataType **kdp)
@@ -289,9 +350,15 @@ void kernelDeinitCuda(LatticeDescType *ld, KernelDataType **kdp)
   *kdp = NULL;
 }
 
+/* the reference's seven names in its order (src/lbm.c:33-41), then the
+ * reduced-precision storage variants */
 const KernelFunctionsType LbmB200Kernels[] = {
   { "cuda-pull-soa", kernelInitCudaPullSoA, kernelDeinitCuda },
+  { "cuda-pull-aos", kernelInitCudaPullAoS, kernelDeinitCuda },
   { "cuda-push-soa", kernelInitCudaPushSoA, kernelDeinitCuda },
+  { "cuda-push-aos", kernelInitCudaPushAoS, kernelDeinitCuda },
+  { "cuda-blk-push-soa", kernelInitCudaBlkPushSoA, kernelDeinitCuda },
+  { "cuda-blk-pull-soa", kernelInitCudaBlkPullSoA, kernelDeinitCuda },
   { "cuda-aa-soa", kernelInitCudaAaSoA, kernelDeinitCuda },
   { "cuda-pull-soa-fp32", kernelInitCudaPullSoAFp32, kernelDeinitCuda },
   { "cuda-push-soa-fp32", kernelInitCudaPushSoAFp32, kernelDeinitCuda },

@@ -494,6 +494,7 @@ class DropIn:
         self.kf = next((k for k in _registry(sp) if k.Name.decode() == name), None)
         if self.kf is None:
             raise KeyError(name)
+        self.aos = "-aos" in name
         L.lbmB200SetBodyForce.argtypes = [ctypes.c_int]
         L.lbmB200SetMagicParameter.argtypes = [ctypes.c_double]
         L.lbmB200SetBodyForce(-1 if force_on is None else int(force_on))
@@ -519,10 +520,14 @@ class DropIn:
         return self.kd.contents
 
     def pdfs(self, which: int) -> np.ndarray:
-        """Zero-copy view of kd->Pdfs[which], shape [19, nx+2, ny+2, nz+2]."""
+        """Zero-copy view of kd->Pdfs[which], shape [19, nx+2, ny+2, nz+2]
+        (indexSoA; for the AoS kernels a transposed view of indexAoS)."""
         g = tuple(self.data.GlobalDims)
         n = Q * g[0] * g[1] * g[2]
-        return np.ctypeslib.as_array(self.data.Pdfs[which], shape=(n,)).reshape((Q,) + g)
+        a = np.ctypeslib.as_array(self.data.Pdfs[which], shape=(n,))
+        if self.aos:
+            return np.moveaxis(a.reshape(g + (Q,)), -1, 0)
+        return a.reshape((Q,) + g)
 
     def set_state(self, f):
         """f[19, nx, ny, nz] for fluid cells, written through kd->SetNode."""

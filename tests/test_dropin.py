@@ -8,6 +8,7 @@ import subprocess
 import pytest
 
 import lbmb200 as L
+import oracle as O
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "lbm-bench_b200")
@@ -57,10 +58,20 @@ def test_single_precision_registry():
     assert L.dropin_kernels(sp=True) == L.dropin_kernels()
 
 
+# the reference's registry (src/lbm.c:33-41)
+REFERENCE_NAMES = ["pull-soa", "pull-aos", "push-soa", "push-aos", "blk-push-soa",
+                   "blk-pull-soa", "aa-soa"]
+
+
 def test_registry_names():
     names = L.dropin_kernels()
-    assert names[:3] == ["cuda-pull-soa", "cuda-push-soa", "cuda-aa-soa"]
-    assert len(names) == 9 and len(set(names)) == 9
+    assert names[:7] == ["cuda-" + n for n in REFERENCE_NAMES]
+    assert len(names) == 13 and len(set(names)) == 13
+
+
+@pytest.mark.skipif(not O.ref_available("plain"), reason="oracle/_ref not built here")
+def test_registry_covers_the_reference_list():
+    assert O.Reference("plain").kernels() == REFERENCE_NAMES
 
 
 def test_cli_lists_kernels_like_the_reference():

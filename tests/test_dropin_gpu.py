@@ -42,6 +42,48 @@ def test_dropin_bit_identical_to_reference_fixtures(golden, case, kernel):
     assert golden_io.state_digest(out, flags) == case["sha256"]
 
 
+LAYOUT_VARIANTS = ["cuda-pull-aos", "cuda-push-aos", "cuda-blk-push-soa", "cuda-blk-pull-soa"]
+SOA_OF = {"cuda-pull-aos": "cuda-pull-soa", "cuda-push-aos": "cuda-push-soa",
+          "cuda-blk-push-soa": "cuda-push-soa", "cuda-blk-pull-soa": "cuda-pull-soa"}
+
+
+@pytest.mark.parametrize("kernel", LAYOUT_VARIANTS)
+@pytest.mark.parametrize("case", STEP_CASES[:6], ids=[c["name"] for c in STEP_CASES[:6]])
+def test_layout_variants_bit_identical_to_reference_fixtures(golden, case, kernel):
+    """The reference's pull-aos / push-aos / blk-*-soa kernels give its SoA
+    kernels' results; so do these names."""
+    _, arrays = golden
+    flags = golden_io.build_flags(case, arrays)
+    f0 = golden_io.initial_state(case, flags)
+    with L.DropIn(kernel, flags, case["periodic"], omega=case["omega"], xforce=case["xforce"],
+                  iterations=case["steps"], force_on=bool(case["force_on"]),
+                  lam=case["lambda"]) as k:
+        k.set_state(f0)
+        k.run()
+        out = k.get_state()
+        assert tuple(k.data.Blk) == ((8, 8, 8) if "blk" in kernel else tuple(k.data.GlobalDims))
+    assert golden_io.state_digest(out, flags) == case["sha256"]
+
+
+@pytest.mark.parametrize("kernel", ["cuda-pull-aos", "cuda-push-aos"])
+@pytest.mark.parametrize("steps", [1, 4])
+def test_aos_host_arrays_are_the_soa_arrays_transposed(kernel, steps):
+    """After Kernel, every slot of both host lattices (ghost layer and the
+    zeros of slots that hold no population included) equals the SoA
+    kernel's, in indexAoS order."""
+    flags, per, _ = L.geometry("blocks-3", (13, 10, 11))
+    f0 = L.perturbed_equilibrium(flags, seed=steps, amplitude=2e-3)
+    arrays = {}
+    for name in (kernel, SOA_OF[kernel]):
+        with L.DropIn(name, flags, per, omega=1.3, iterations=steps, force_on=True) as k:
+            k.set_state(f0)
+            k.run()
+            # DropIn.pdfs reads the AoS kernel's arrays in indexAoS order
+            arrays[name] = [k.pdfs(b).copy() for b in (0, 1)]
+    for b in (0, 1):
+        assert np.array_equal(arrays[kernel][b], arrays[SOA_OF[kernel]][b])
+
+
 def test_dropin_ends_in_the_buffer_the_reference_ends_in():
     flags, per, _ = L.geometry("channel", (10, 9, 8))
     f0 = L.perturbed_equilibrium(flags, seed=3)
@@ -113,7 +155,7 @@ def test_cli_verification_run_succeeds(kernel):
     assert r.returncode == 0, r.stdout + r.stderr
     assert "# VERIFICATION SUCCEEDED." in r.stdout
     err = float(re.search(r"deviation from analytical solution: (\S+)", r.stdout).group(1))
-    if kernel in ("cuda-pull-soa", "cuda-push-soa", "cuda-aa-soa"):
+    if not kernel.endswith(("-fp32", "-fp16")):
         # the reference's own -V run on this case gives 4.5614e-02 (golden fixture)
         ref = next(c for c in CASES if c["name"] == "poiseuille_V")["verify"]["aa-soa"]
         assert err == pytest.approx(ref["error_norm"], rel=1e-6)
