@@ -6,21 +6,31 @@
 #include "lbm_internal.h"
 #include "lbm_step_x2.cuh"
 #include "lbm_step_x2s.cuh"
+#include "lbm_step_x4s.cuh"
 
 namespace lbm {
 
-// The shuffle-aligned kernel serves the shifted patterns when nz is a
-// multiple of 64; AA even in FP16 storage takes the four-cell kernel; the
-// rest uses the generic two-cell kernel.
+// In FP16 storage without the Brinkman term the four-cell kernels serve AA
+// even (pz % 4 == 0) and AA odd (nz a multiple of 128). The shuffle-aligned
+// two-cell kernel serves the other shifted steps when nz is a multiple of
+// 64; the rest uses the generic two-cell kernel.
 template <class ST, int KIND, bool FORCE, bool BRINK>
 static cudaError_t go(const StepArgs2<ST> &a, dim3 grid, dim3 block, cudaStream_t st)
 {
-  if constexpr (std::is_same<ST, StoreF16>::value && KIND == kAAEvenStep && !BRINK) {
-    if (a.g.pz % 4 == 0 && !a.no_quad) {
+  if constexpr (std::is_same<ST, StoreF16>::value && !BRINK) {
+    if (KIND == kAAEvenStep && a.g.pz % 4 == 0 && !a.no_quad) {
       dim3 qg, qb;
       quad_launch_shape(a.g, qg, qb);
       step_kernel_even_quad<FORCE><<<qg, qb, 0, st>>>(a);
       return cudaGetLastError();
+    }
+    if constexpr (KIND == kAAOddStep) {
+      if (a.g.nz % 128 == 0 && !a.no_quad && !a.no_shuffle) {
+        dim3 qg, qb;
+        quad_shuffle_launch_shape(a.g, qg, qb);
+        step_kernel_x4s<KIND, FORCE><<<qg, qb, 0, st>>>(a);
+        return cudaGetLastError();
+      }
     }
   }
   if (KIND != kAAEvenStep && a.g.nz % 64 == 0 && !a.no_shuffle) {

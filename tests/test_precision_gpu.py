@@ -128,6 +128,30 @@ def test_fp16_four_cell_even_kernel_equals_pair_kernel(monkeypatch, dims, per):
         assert np.array_equal(outs[0], outs[1]), steps
 
 
+@pytest.mark.parametrize("dims", [(9, 11, 128), (6, 5, 256)])
+@pytest.mark.parametrize("per", [(1, 0, 0), (1, 1, 1), (0, 1, 1)])
+def test_fp16_four_cell_shifted_kernels_equal_pair_kernels(monkeypatch, dims, per):
+    """For nz a multiple of 128 the FP16 pull, push and AA odd steps run the
+    four-cells-per-thread shuffle kernel; it collides the two pairs with the
+    pair kernels' arithmetic, so the states agree bit for bit with
+    LBM_B200_NO_QUAD=1 (the two-cell shuffle kernel): walled and periodic z,
+    force, odd and even step counts."""
+    rng = np.random.default_rng(sum(dims) + sum(per))
+    flags = _random_walls(rng, dims, per, solid=0.3)
+    f0 = L.perturbed_equilibrium(flags, seed=6, amplitude=2e-3)
+    for pattern in ("aa", "pull", "push"):
+        for steps in (1, 4, 7):
+            outs = []
+            for no_quad in ("0", "1"):
+                monkeypatch.setenv("LBM_B200_NO_QUAD", no_quad)
+                with L.Solver(flags, per, pattern, L.F16) as s:
+                    s.set_params(1.3, 3 / 16, 1e-5, steps != 4)
+                    s.set_state(f0)
+                    s.run(steps)
+                    outs.append(s.get_state())
+            assert np.array_equal(outs[0], outs[1]), (pattern, steps)
+
+
 @pytest.mark.parametrize("per", [(1, 0, 0), (1, 1, 1)])
 def test_shuffle_aligned_kernels_track_the_oracle(oracle, per):
     import oracle as O
