@@ -161,6 +161,25 @@ int lbm_halo_unpack(lbm_solver *s, int when, const void *from_left, const void *
 /* The solver's CUDA stream (cudaStream_t), for ordering a transport on it. */
 void *lbm_stream(const lbm_solver *s);
 
+/* One step split into ranges of x planes, so that a slab's interior update
+ * overlaps its halo exchange (no reference counterpart: LBM-Bench has no
+ * decomposition). lbm_step_begin opens the step and forks a second stream
+ * after the work queued on the solver's stream; lbm_step_planes launches
+ * the step on the solver's own planes [x_begin, x_end) (0 <= x_begin <
+ * x_end <= nx, each plane once per step) on the solver's stream (on_side =
+ * 0) or on the second stream (on_side = 1); lbm_step_end checks that every
+ * plane was launched, joins the second stream into the solver's stream and
+ * advances the step. Halo packs and unpacks between begin and end run on
+ * the solver's stream. For a slab the exchanged slots and the interior
+ * planes 1 .. nx-2 touch disjoint memory: the interior can run on the side
+ * stream while the solver's stream packs, exchanges and unpacks the BEFORE
+ * messages, updates planes 0 and nx-1, and exchanges the AFTER messages.
+ * Results are bit-identical to lbm_run(s, 1). While a step is open,
+ * lbm_run, the state transfers and the adjoint return LBM_ERR_STATE. */
+int lbm_step_begin(lbm_solver *s);
+int lbm_step_planes(lbm_solver *s, int x_begin, int x_end, int on_side);
+int lbm_step_end(lbm_solver *s);
+
 /* Sets the state on the device to the seeded initial condition of
  * lbm_perturbed_equilibrium (identical values, no host array): for domains
  * whose FP64 host state would not fit in host memory. */

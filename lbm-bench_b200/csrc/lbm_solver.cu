@@ -81,6 +81,12 @@ struct lbm_solver {
   uint8_t *bc_marks;     // [2][ny][nz]: inlet / outlet cells of the pressure boundary, or NULL
   int bc_on;
   double rho_in, rho_out;
+  // split steps (lbm_step_begin / _planes / _end)
+  cudaStream_t side;     // second stream, created on first use
+  cudaEvent_t fork_ev, join_ev;
+  int split;             // a split step is open
+  uint8_t *split_done;   // host: x planes of the open step already launched (nx bytes)
+  int split_left;        // planes still to launch
 };
 
 extern "C" const char *lbm_last_error(void) { return g_err; }
@@ -495,6 +501,13 @@ static void free_all(lbm_solver *s)
   cudaFree(s->red);
   cudaFree(s->dev_err);
   cudaFree(s->bc_marks);
+  free(s->split_done);
+  if (s->fork_ev)
+    cudaEventDestroy(s->fork_ev);
+  if (s->join_ev)
+    cudaEventDestroy(s->join_ev);
+  if (s->side)
+    cudaStreamDestroy(s->side);
   if (s->ev[0])
     cudaEventDestroy(s->ev[0]);
   if (s->ev[1])
@@ -627,7 +640,15 @@ static int create_impl(lbm_solver **out, int nx, int ny, int nz, const int *flag
     }                                                                                       \
   } while (0)
 
-  TRYC(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  if (slab) {
+    // a slab's stream carries the halo exchange and the boundary planes of
+    // split steps: it outranks the second stream with the interior planes
+    int least = 0, greatest = 0;
+    TRYC(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    TRYC(cudaStreamCreateWithPriority(&s->stream, cudaStreamNonBlocking, greatest));
+  } else {
+    TRYC(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  }
   TRYC(cudaEventCreate(&s->ev[0]));
   TRYC(cudaEventCreate(&s->ev[1]));
   TRY(dev_alloc(s, &s->buf[0], s->state_bytes, "the population lattice"));
@@ -863,6 +884,8 @@ extern "C" int lbm_set_state(lbm_solver *s, const double *f)
 {
   if (!s || !f)
     return fail(LBM_ERR_ARG, "lbm_set_state: NULL argument");
+  if (s->split)
+    return fail(LBM_ERR_STATE, "lbm_set_state: a split step is open");
   CUDA_TRY(cudaSetDevice(s->device));
   switch (s->precision) {
   case LBM_F64: return pack_all<StoreF64>(s, f);
@@ -875,6 +898,8 @@ extern "C" int lbm_get_state(lbm_solver *s, double *f)
 {
   if (!s || !f)
     return fail(LBM_ERR_ARG, "lbm_get_state: NULL argument");
+  if (s->split)
+    return fail(LBM_ERR_STATE, "lbm_get_state: a split step is open");
   CUDA_TRY(cudaSetDevice(s->device));
   switch (s->precision) {
   case LBM_F64: return unpack_all<StoreF64>(s, f);
@@ -1112,6 +1137,8 @@ static int ref_dispatch(lbm_solver *s, void *host, int elem_size, int ref_orient
   if (!s || !host || (elem_size != 8 && elem_size != 4) || o < LBM_REF_NATURAL ||
       o > LBM_REF_AA_EVEN)
     return fail(LBM_ERR_ARG, "padded transfer: bad arguments");
+  if (s->split)
+    return fail(LBM_ERR_STATE, "padded transfer: a split step is open");
   CUDA_TRY(cudaSetDevice(s->device));
   if (elem_size == 8) {
     if (s->precision == LBM_F64)
@@ -1139,11 +1166,15 @@ extern "C" int lbm_get_state_padded(lbm_solver *s, void *pdfs, int elem_size,
   return ref_dispatch(s, pdfs, elem_size, ref_orientation, false);
 }
 
-// Launches one step and advances the bookkeeping.
-static int launch_one(lbm_solver *s, int *kind_out)
+// Launches the step kernel of the next step over device x planes
+// [x0, x0 + planes) on stream st, without advancing the bookkeeping. The
+// pipelined FP64 kernels only serve whole steps.
+static int launch_kernel(lbm_solver *s, int x0, int planes, cudaStream_t st, int *kind_out)
 {
   dim3 grid, block;
   cell_launch_shape(s->g, grid, block);
+  grid.z = planes;
+  const bool whole = x0 == 0 && planes == s->g.nx;
   int kind;
   const void *src;
   void *dst;
@@ -1167,7 +1198,8 @@ static int launch_one(lbm_solver *s, int *kind_out)
     a.porosity = s->porosity;
     a.u_save = brink ? (double *)s->u_save_next : nullptr;
     a.c = make_consts<double>(s);
-    if (s->tma && !brink) {
+    a.x0 = x0;
+    if (s->tma && !brink && whole) {
       TmaArgs<StoreF64> t;
       t.s = a;
       t.T = s->tma_shape.T;
@@ -1176,9 +1208,9 @@ static int launch_one(lbm_solver *s, int *kind_out)
       t.ntiles = s->tma_shape.ntiles;
       t.stage_bytes = s->tma_shape.stage_bytes;
       t.err = s->dev_err;
-      e = launch_step_tma_f64(kind, force, t, s->tma_groups, s->tma_shape.blocks, s->stream);
+      e = launch_step_tma_f64(kind, force, t, s->tma_groups, s->tma_shape.blocks, st);
     } else {
-      e = launch_step_f64(kind, force, brink, a, grid, block, s->stream);
+      e = launch_step_f64(kind, force, brink, a, grid, block, st);
     }
   } else if (s->precision == LBM_F32) {
     StepArgs2<StoreF32> a;
@@ -1191,7 +1223,9 @@ static int launch_one(lbm_solver *s, int *kind_out)
     a.c = make_consts2(s);
     a.no_shuffle = s->no_shuffle;
     a.no_quad = s->no_quad;
-    e = launch_step_x2_f32(kind, force, brink, a, s->stream);
+    a.x0 = x0;
+    a.planes = planes;
+    e = launch_step_x2_f32(kind, force, brink, a, st);
   } else {
     StepArgs2<StoreF16> a;
     a.g = s->g;
@@ -1203,17 +1237,27 @@ static int launch_one(lbm_solver *s, int *kind_out)
     a.c = make_consts2(s);
     a.no_shuffle = s->no_shuffle;
     a.no_quad = s->no_quad;
-    e = launch_step_x2_f16(kind, force, brink, a, s->stream);
+    a.x0 = x0;
+    a.planes = planes;
+    e = launch_step_x2_f16(kind, force, brink, a, st);
   }
   if (e != cudaSuccess)
     return fail(LBM_ERR_CUDA, "step launch failed: %s", cudaGetErrorString(e));
-  if (s->pattern != LBM_AA)
-    s->cur ^= 1;
-  s->steps_done++;
   s->launches++;
   if (kind_out)
     *kind_out = kind;
+  return LBM_OK;
+}
+
+// After all planes of a step: the lattice swap and step count, then the
+// pressure boundary of the new state.
+static int finish_step(lbm_solver *s)
+{
+  if (s->pattern != LBM_AA)
+    s->cur ^= 1;
+  s->steps_done++;
   if (s->bc_on) {
+    cudaError_t e;
     e = launch_pressure_bc(s->precision, s->g, s->ub, orientation(s), (void *)state_ptr(s),
         s->mask, s->bc_marks, s->rho_in, s->rho_out,
         (float)(s->precision == LBM_F16 ? s->fp16_scale : 1.0), s->stream);
@@ -1221,6 +1265,85 @@ static int launch_one(lbm_solver *s, int *kind_out)
       return fail(LBM_ERR_CUDA, "pressure boundary launch failed: %s", cudaGetErrorString(e));
   }
   return LBM_OK;
+}
+
+// Launches one whole step and advances the bookkeeping.
+static int launch_one(lbm_solver *s, int *kind_out)
+{
+  if (s->split)
+    return fail(LBM_ERR_STATE, "a split step is open (lbm_step_begin without lbm_step_end)");
+  int rc = launch_kernel(s, 0, s->g.nx, s->stream, kind_out);
+  return rc ? rc : finish_step(s);
+}
+
+extern "C" int lbm_step_begin(lbm_solver *s)
+{
+  if (!s)
+    return fail(LBM_ERR_ARG, "lbm_step_begin: NULL solver");
+  if (s->split)
+    return fail(LBM_ERR_STATE, "lbm_step_begin: a split step is already open");
+  CUDA_TRY(cudaSetDevice(s->device));
+  if (!s->side) {
+    int least = 0, greatest = 0;
+    CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    CUDA_TRY(cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, least));
+    CUDA_TRY(cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming));
+  }
+  if (!s->split_done) {
+    s->split_done = (uint8_t *)malloc((size_t)s->nx);
+    if (!s->split_done)
+      return fail(LBM_ERR_ALLOC, "lbm_step_begin: host allocation failed");
+  }
+  memset(s->split_done, 0, (size_t)s->nx);
+  s->split_left = s->nx;
+  // the side stream starts after everything queued on the solver's stream
+  CUDA_TRY(cudaEventRecord(s->fork_ev, s->stream));
+  CUDA_TRY(cudaStreamWaitEvent(s->side, s->fork_ev, 0));
+  s->split = 1;
+  return LBM_OK;
+}
+
+extern "C" int lbm_step_planes(lbm_solver *s, int x_begin, int x_end, int on_side)
+{
+  if (!s)
+    return fail(LBM_ERR_ARG, "lbm_step_planes: NULL solver");
+  if (!s->split)
+    return fail(LBM_ERR_STATE, "lbm_step_planes: no split step open (lbm_step_begin)");
+  if (x_begin < 0 || x_end > s->nx || x_begin >= x_end)
+    return fail(LBM_ERR_ARG, "lbm_step_planes: planes [%d, %d) outside [0, %d)", x_begin, x_end,
+        s->nx);
+  for (int x = x_begin; x < x_end; ++x)
+    if (s->split_done[x])
+      return fail(LBM_ERR_ARG, "lbm_step_planes: plane %d already updated in this step", x);
+  CUDA_TRY(cudaSetDevice(s->device));
+  int rc = launch_kernel(s, x_begin + s->ub.ox, x_end - x_begin, on_side ? s->side : s->stream,
+      NULL);
+  if (rc)
+    return rc;
+  memset(s->split_done + x_begin, 1, (size_t)(x_end - x_begin));
+  s->split_left -= x_end - x_begin;
+  return LBM_OK;
+}
+
+extern "C" int lbm_step_end(lbm_solver *s)
+{
+  if (!s)
+    return fail(LBM_ERR_ARG, "lbm_step_end: NULL solver");
+  if (!s->split)
+    return fail(LBM_ERR_STATE, "lbm_step_end: no split step open (lbm_step_begin)");
+  if (s->split_left) {
+    int x = 0;
+    while (x < s->nx && s->split_done[x])
+      ++x;
+    return fail(LBM_ERR_STATE, "lbm_step_end: %d plane(s) not updated, the first is %d",
+        s->split_left, x);
+  }
+  CUDA_TRY(cudaSetDevice(s->device));
+  CUDA_TRY(cudaEventRecord(s->join_ev, s->side));
+  CUDA_TRY(cudaStreamWaitEvent(s->stream, s->join_ev, 0));
+  s->split = 0;
+  return finish_step(s);
 }
 
 extern "C" int lbm_set_pressure_bc(lbm_solver *s, double rho_in, double rho_out, int on)
@@ -1274,6 +1397,8 @@ extern "C" int lbm_synchronize(lbm_solver *s)
   if (!s)
     return fail(LBM_ERR_ARG, "lbm_synchronize: NULL solver");
   CUDA_TRY(cudaStreamSynchronize(s->stream));
+  if (s->side)
+    CUDA_TRY(cudaStreamSynchronize(s->side));
   return check_kernel_error(s);
 }
 
@@ -1550,12 +1675,21 @@ __global__ void halo_copy_kernel(Grid g, UserBox u, int xplane, int sgn, T *stat
   state[si] = buf[bi];
 }
 
-static int halo_copy(lbm_solver *s, int xplane, int sgn, void *buf, int to_buf,
+// The lattice an exchange reads and writes: the state, except for an
+// after-step exchange inside a split step of pull / push, whose messages are
+// in the lattice the open step writes (the lattices swap at lbm_step_end).
+static void *halo_lattice(const lbm_solver *s, int when)
+{
+  if (s->pattern == LBM_AA)
+    return s->buf[0];
+  return s->buf[s->cur ^ ((s->split && when == LBM_HALO_AFTER) ? 1 : 0)];
+}
+
+static int halo_copy(lbm_solver *s, void *st, int xplane, int sgn, void *buf, int to_buf,
     int guarded = 0)
 {
   dim3 block(32, 8, 1);
   dim3 grid((s->ub.nz + 31) / 32, (s->ub.ny + 7) / 8, 5);
-  void *st = s->pattern == LBM_AA ? s->buf[0] : s->buf[s->cur];
   switch (storage_size(s->precision)) {
   case 8:
     halo_copy_kernel<uint64_t><<<grid, block, 0, s->stream>>>(s->g, s->ub, xplane, sgn,
@@ -1605,16 +1739,18 @@ static int halo_check(const lbm_solver *s, int when, const void *a, const void *
     return fail(LBM_ERR_ARG, "%s: when = %d is not LBM_HALO_BEFORE, _AFTER or _SCATTER", fn,
         when);
   // before: the next step's needs (and a shifted state's ghost data, which
-  // are the same slots); after: the last step's; scatter: shifted states
+  // are the same slots); after: the last step's, or the open split step's;
+  // scatter: shifted states, outside split steps
+  const long long done = s->steps_done + ((s->split && when == LBM_HALO_AFTER) ? 1 : 0);
   bool ok;
   if (when == LBM_HALO_SCATTER)
-    ok = lbm_halo_shifted(s);
+    ok = lbm_halo_shifted(s) && !s->split;
   else if (s->pattern == LBM_PULL)
     ok = when == LBM_HALO_BEFORE;
   else if (s->pattern == LBM_PUSH)
     ok = when == LBM_HALO_AFTER;
   else
-    ok = when == LBM_HALO_BEFORE ? (s->steps_done & 1) : (s->steps_done > 0 && !(s->steps_done & 1));
+    ok = when == LBM_HALO_BEFORE ? (s->steps_done & 1) : (done > 0 && !(done & 1));
   if (!ok)
     return fail(LBM_ERR_STATE, "%s: no %s exchange at step %lld of this pattern", fn,
         when == LBM_HALO_BEFORE ? "before-step" : when == LBM_HALO_AFTER ? "after-step" :
@@ -1628,22 +1764,23 @@ extern "C" int lbm_halo_pack(lbm_solver *s, int when, void *to_left, void *to_ri
   int rc = halo_check(s, when, to_left, to_right, "lbm_halo_pack");
   if (rc)
     return rc;
+  void *lat = halo_lattice(s, when);
   const int first = 1, last = s->g.nx - 2;
   // slots of a shifted state in the left ghost: pull P, AA M (right: opposite)
   const int left_ghost_set = s->pattern == LBM_PULL ? +1 : -1;
   if (when == LBM_HALO_BEFORE) {
-    if ((rc = halo_copy(s, last, left_ghost_set, to_right, 1)))
+    if ((rc = halo_copy(s, lat, last, left_ghost_set, to_right, 1)))
       return rc;
-    return halo_copy(s, first, -left_ghost_set, to_left, 1);
+    return halo_copy(s, lat, first, -left_ghost_set, to_left, 1);
   }
   if (when == LBM_HALO_SCATTER) {
-    if ((rc = halo_copy(s, 0, left_ghost_set, to_left, 1)))
+    if ((rc = halo_copy(s, lat, 0, left_ghost_set, to_left, 1)))
       return rc;
-    return halo_copy(s, s->g.nx - 1, -left_ghost_set, to_right, 1);
+    return halo_copy(s, lat, s->g.nx - 1, -left_ghost_set, to_right, 1);
   }
-  if ((rc = halo_copy(s, s->g.nx - 1, +1, to_right, 1)))
+  if ((rc = halo_copy(s, lat, s->g.nx - 1, +1, to_right, 1)))
     return rc;
-  return halo_copy(s, 0, -1, to_left, 1);
+  return halo_copy(s, lat, 0, -1, to_left, 1);
 }
 
 extern "C" int lbm_halo_unpack(lbm_solver *s, int when, const void *from_left,
@@ -1652,26 +1789,27 @@ extern "C" int lbm_halo_unpack(lbm_solver *s, int when, const void *from_left,
   int rc = halo_check(s, when, from_left, from_right, "lbm_halo_unpack");
   if (rc)
     return rc;
+  void *lat = halo_lattice(s, when);
   const int first = 1, last = s->g.nx - 2;
   const int left_ghost_set = s->pattern == LBM_PULL ? +1 : -1;
   if (when == LBM_HALO_BEFORE) {
     // the left slab sent its last plane's slots of our left ghost's set
-    if ((rc = halo_copy(s, 0, left_ghost_set, (void *)from_left, 0)))
+    if ((rc = halo_copy(s, lat, 0, left_ghost_set, (void *)from_left, 0)))
       return rc;
-    return halo_copy(s, s->g.nx - 1, -left_ghost_set, (void *)from_right, 0);
+    return halo_copy(s, lat, s->g.nx - 1, -left_ghost_set, (void *)from_right, 0);
   }
   if (when == LBM_HALO_SCATTER) {
     // the left slab sent its right ghost (our first plane's share of its
     // boundary cells' populations); the pull state keeps population d of
     // x + c_d in slot d of x, the AA state population inv d of x - c_d
     const int gm = s->pattern == LBM_PULL ? kGuardOwn : kGuardInv;
-    if ((rc = halo_copy(s, first, -left_ghost_set, (void *)from_left, 0, gm)))
+    if ((rc = halo_copy(s, lat, first, -left_ghost_set, (void *)from_left, 0, gm)))
       return rc;
-    return halo_copy(s, last, left_ghost_set, (void *)from_right, 0, gm);
+    return halo_copy(s, lat, last, left_ghost_set, (void *)from_right, 0, gm);
   }
-  if ((rc = halo_copy(s, first, +1, (void *)from_left, 0, kGuardInv)))
+  if ((rc = halo_copy(s, lat, first, +1, (void *)from_left, 0, kGuardInv)))
     return rc;
-  return halo_copy(s, last, -1, (void *)from_right, 0, kGuardInv);
+  return halo_copy(s, lat, last, -1, (void *)from_right, 0, kGuardInv);
 }
 
 extern "C" void *lbm_stream(const lbm_solver *s) { return s ? (void *)s->stream : NULL; }
@@ -1817,6 +1955,8 @@ extern "C" int lbm_adjoint_gradient(lbm_solver *s, int steps, int checkpoint_eve
 {
   if (!s || steps < 1 || !grad)
     return fail(LBM_ERR_ARG, "lbm_adjoint_gradient: bad arguments");
+  if (s->split)
+    return fail(LBM_ERR_STATE, "lbm_adjoint_gradient: a split step is open");
   if (s->pattern != LBM_AA)
     return fail(LBM_ERR_ARG, "lbm_adjoint_gradient: needs an AA solver");
   if (s->slab)

@@ -49,6 +49,7 @@ template <class ST> struct StepArgs {
   const float *porosity; // Brinkman only
   V *u_save;             // Brinkman only, optional: momentum per cell (3 planes)
   Consts<V> c;
+  int x0 = 0;            // first storage x plane of the launch (grid.z planes from there)
 };
 
 // Minimum resident blocks per SM requested from the compiler (caps the
@@ -94,7 +95,7 @@ __global__ void __launch_bounds__(kStepThreads, (StepOccupancy<ST, KIND>::value)
   const Grid &g = a.g;
   const int z = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int x = blockIdx.z;
+  const int x = a.x0 + (int)blockIdx.z;
   if (z >= g.nz || y >= g.ny)
     return;
   const uint32_t cell = cell_index(g, x, y, z);

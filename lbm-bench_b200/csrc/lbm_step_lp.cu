@@ -21,6 +21,7 @@ static cudaError_t go(const StepArgs2<ST> &a, dim3 grid, dim3 block, cudaStream_
     if (KIND == kAAEvenStep && a.g.pz % 4 == 0 && !a.no_quad) {
       dim3 qg, qb;
       quad_launch_shape(a.g, qg, qb);
+      qg.z = a.planes;
       step_kernel_even_quad<FORCE><<<qg, qb, 0, st>>>(a);
       return cudaGetLastError();
     }
@@ -28,6 +29,7 @@ static cudaError_t go(const StepArgs2<ST> &a, dim3 grid, dim3 block, cudaStream_
       if (a.g.nz % 128 == 0 && !a.no_quad && !a.no_shuffle) {
         dim3 qg, qb;
         quad_shuffle_launch_shape(a.g, qg, qb);
+        qg.z = a.planes;
         step_kernel_x4s<KIND, FORCE><<<qg, qb, 0, st>>>(a);
         return cudaGetLastError();
       }
@@ -36,6 +38,7 @@ static cudaError_t go(const StepArgs2<ST> &a, dim3 grid, dim3 block, cudaStream_
   if (KIND != kAAEvenStep && a.g.nz % 64 == 0 && !a.no_shuffle) {
     dim3 sg, sb;
     shuffle_launch_shape(a.g, sg, sb);
+    sg.z = a.planes;
     step_kernel_x2s<ST, KIND, FORCE, BRINK><<<sg, sb, 0, st>>>(a);
   } else {
     step_kernel_x2<ST, KIND, FORCE, BRINK><<<grid, block, 0, st>>>(a);
@@ -59,6 +62,7 @@ static cudaError_t launch(int kind, bool force, bool brink, const StepArgs2<ST> 
 {
   dim3 grid, block;
   pair_launch_shape(a.g, grid, block);
+  grid.z = a.planes;
   switch (kind) {
   case kPullStep: return pick<ST, kPullStep>(force, brink, a, grid, block, st);
   case kPushStep: return pick<ST, kPushStep>(force, brink, a, grid, block, st);

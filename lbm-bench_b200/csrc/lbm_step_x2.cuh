@@ -124,6 +124,8 @@ template <class ST> struct StepArgs2 {
   Consts2 c;
   int no_shuffle; // host-side switch: use the generic two-cell kernel only
   int no_quad;    // host-side switch: AA even in FP16 storage on the two-cell kernel
+  int x0 = 0;     // first storage x plane of the launch (grid.z planes from there)
+  int planes = 0; // x planes of the launch
 };
 
 // Minimum resident CTAs per SM of the pair kernels, per storage type and
@@ -149,7 +151,7 @@ __global__ void __launch_bounds__(kStepThreads, (PairOccupancy<ST, KIND, false>:
   const Grid &g = a.g;
   const int z = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int x = blockIdx.z;
+  const int x = a.x0 + (int)blockIdx.z;
   if (z >= g.nz || y >= g.ny)
     return;
   // the pair starts on an even element (pz is even), so pair
@@ -290,7 +292,7 @@ __global__ void __launch_bounds__(kStepThreads, LBM_MINB_QUAD)
   const Grid &g = a.g;
   const int z = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int x = blockIdx.z;
+  const int x = a.x0 + (int)blockIdx.z;
   if (z >= g.nz || y >= g.ny)
     return;
   const long long PL = g.plane;

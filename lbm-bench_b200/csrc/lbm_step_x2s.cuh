@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(kStepThreads, (PairOccupancy<ST, KIND, true>::
   const int lane = threadIdx.x; // blockDim.x == 32
   const int z = 64 * blockIdx.x + 2 * lane;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int x = blockIdx.z;
+  const int x = a.x0 + (int)blockIdx.z;
   if (y >= g.ny) // uniform across the warp
     return;
   const uint32_t cell = cell_index(g, x, y, z);

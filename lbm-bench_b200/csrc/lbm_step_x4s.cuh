@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(kStepThreads, LBM_MINB_X4S)
   const int lane = threadIdx.x; // blockDim.x == 32
   const int z = 128 * blockIdx.x + 4 * lane;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int x = blockIdx.z;
+  const int x = a.x0 + (int)blockIdx.z;
   if (y >= g.ny) // uniform across the warp
     return;
   const uint32_t cell = cell_index(g, x, y, z);

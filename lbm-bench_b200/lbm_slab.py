@@ -96,15 +96,23 @@ class SlabRunner:
     """Steps one slab of a ring: exchange, step, exchange, as the pattern
     and the step parity need (Solver.halo_needs).
 
-    `solver` is a slab (Solver.slab) or any object with the same halo_*
-    methods, run() and stream; `device` is where the message buffers live
-    ("cuda" for a GPU slab)."""
+    With overlap=True each step is split (Solver.step_begin / step_planes /
+    step_end): the interior planes 1 .. nx-2 run on the solver's second
+    stream while its own stream packs, exchanges and unpacks the BEFORE
+    messages, updates the boundary planes 0 and nx-1 and exchanges the AFTER
+    messages. The exchanged slots and the interior touch disjoint memory, so
+    the result is the same bit for bit.
 
-    def __init__(self, solver, ring: Ring, device="cuda"):
+    `solver` is a slab (Solver.slab) or any object with the same halo_*
+    methods, run(), the step_* methods (for overlap), shape and stream;
+    `device` is where the message buffers live ("cuda" for a GPU slab)."""
+
+    def __init__(self, solver, ring: Ring, device="cuda", overlap=False):
         import torch
         self.torch = torch
         self.s = solver
         self.ring = ring
+        self.overlap = overlap
         n = solver.halo_bytes
         if n <= 0:
             raise ValueError("SlabRunner needs a slab solver (lbm_create_slab)")
@@ -131,11 +139,29 @@ class SlabRunner:
     def run(self, steps: int):
         for _ in range(steps):
             need = self.s.halo_needs
+            if self.overlap:
+                self._split_step(need)
+                continue
             if need & L.HALO_BEFORE:
                 self._exchange(L.HALO_BEFORE)
             self.s.run(1)
             if need & L.HALO_AFTER:
                 self._exchange(L.HALO_AFTER)
+
+    def _split_step(self, need: int):
+        s = self.s
+        nx = s.shape[0]
+        s.step_begin()
+        if nx > 2:
+            s.step_planes(1, nx - 1, side=True)
+        if need & L.HALO_BEFORE:
+            self._exchange(L.HALO_BEFORE)
+        s.step_planes(0, 1)
+        if nx > 1:
+            s.step_planes(nx - 1, nx)
+        if need & L.HALO_AFTER:
+            self._exchange(L.HALO_AFTER)
+        s.step_end()
 
     def gather(self):
         """Before reading the state: the neighbours' share of this slab's
@@ -156,8 +182,9 @@ class LocalRing:
     messages. For tests and for domains split over the devices of one
     process; the kernels of different slabs never wait on one another."""
 
-    def __init__(self, solvers, device="cuda"):
+    def __init__(self, solvers, device="cuda", overlap=False):
         import torch
+        self.overlap = overlap
         self.solvers = list(solvers)
         self.bufs = []
         for s in self.solvers:
@@ -184,12 +211,25 @@ class LocalRing:
             if len(needs) != 1:
                 raise RuntimeError("slabs of one ring are at different steps")
             need = needs.pop()
+            if self.overlap:  # the schedule of SlabRunner(overlap=True)
+                for s in self.solvers:
+                    s.step_begin()
+                    if s.shape[0] > 2:
+                        s.step_planes(1, s.shape[0] - 1, side=True)
             if need & L.HALO_BEFORE:
                 self._exchange(L.HALO_BEFORE)
             for s in self.solvers:
-                s.run(1)
+                if self.overlap:
+                    s.step_planes(0, 1)
+                    if s.shape[0] > 1:
+                        s.step_planes(s.shape[0] - 1, s.shape[0])
+                else:
+                    s.run(1)
             if need & L.HALO_AFTER:
                 self._exchange(L.HALO_AFTER)
+            if self.overlap:
+                for s in self.solvers:
+                    s.step_end()
 
     def gather(self):
         """Before reading the slabs' states (see SlabRunner.gather)."""

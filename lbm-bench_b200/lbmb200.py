@@ -58,6 +58,9 @@ _SIGNATURES = [
     ("lbm_halo_pack", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     ("lbm_halo_unpack", ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp]),
     ("lbm_stream", _vp, [_vp]),
+    ("lbm_step_begin", ctypes.c_int, [_vp]),
+    ("lbm_step_planes", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    ("lbm_step_end", ctypes.c_int, [_vp]),
     ("lbm_destroy", ctypes.c_int, [_vp]),
     ("lbm_set_params", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                       ctypes.c_int]),
@@ -213,6 +216,18 @@ class Solver:
     def stream(self) -> int:
         """The solver's cudaStream_t as an integer."""
         return lib().lbm_stream(self._h) or 0
+
+    # -- split steps (lbm_step_begin / _planes / _end) ----------------------
+    def step_begin(self) -> None:
+        _check(lib().lbm_step_begin(self._h))
+
+    def step_planes(self, x_begin: int, x_end: int, side: bool = False) -> None:
+        """Launches the open step on own planes [x_begin, x_end), on the
+        solver's stream or (side=True) on its second stream."""
+        _check(lib().lbm_step_planes(self._h, x_begin, x_end, int(side)))
+
+    def step_end(self) -> None:
+        _check(lib().lbm_step_end(self._h))
 
     # -- lifecycle ---------------------------------------------------------
     def close(self) -> None:

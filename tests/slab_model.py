@@ -61,9 +61,14 @@ class _Lattice:
         raise NotImplementedError
 
     def step(self):
+        self._update(self.own)
+        self._advance()
+
+    def _update(self, xs):
+        """Updates the cells of storage planes xs for the next step (no
+        lattice swap, no step count)."""
         fl = self.fluid
         nxd, ny, nz = fl.shape
-        xs = self.own
         X, Y, Z = np.meshgrid(xs, np.arange(ny), np.arange(nz), indexing="ij")
         live = fl[X, Y, Z]
         X, Y, Z = X[live], Y[live], Z[live]
@@ -106,6 +111,9 @@ class _Lattice:
                     wall = ~fl[tx, ty, tz]
                     dst[INV[d], X[wall], Y[wall], Z[wall]] = out[d][wall]
                     dst[d, tx[~wall], ty[~wall], tz[~wall]] = out[d][~wall]
+
+    def _advance(self):
+        if self.pattern != "aa":
             self.cur ^= 1
         self.steps_done += 1
 
@@ -165,15 +173,21 @@ class Slab(_Lattice):
             return (first, ls), (last, rs), (gl, rs), (gr, ls)
         return (gl, MINUS), (gr, PLUS), (first, PLUS), (last, MINUS)
 
+    def _lattice(self, when):
+        # an after-step exchange inside a split step: the lattice being written
+        if self.pattern != "aa" and when == HALO_AFTER and getattr(self, "_open", None) is not None:
+            return self.buf[self.cur ^ 1]
+        return self.state
+
     def halo_pack(self, when, to_left, to_right):
         (pl, sl), (pr, sr), _, _ = self._plan(when)
-        st = self.state
+        st = self._lattice(when)
         to_left.numpy().view(np.float64)[:] = st[sl, pl].ravel()
         to_right.numpy().view(np.float64)[:] = st[sr, pr].ravel()
 
     def halo_unpack(self, when, from_left, from_right):
         _, _, (ul, sl), (ur, sr) = self._plan(when)
-        st = self.state
+        st = self._lattice(when)
         shp = (5,) + st.shape[2:]
         for x, sset, msg in ((ul, sl, from_left), (ur, sr, from_right)):
             m = msg.numpy().view(np.float64).reshape(shp)
@@ -189,3 +203,22 @@ class Slab(_Lattice):
 
     def own_state(self):
         return self.state[:, 1:self.nx + 1]
+
+    # split steps: planes update at once, in call order
+    def step_begin(self):
+        assert getattr(self, "_open", None) is None
+        self._open = np.zeros(self.nx, dtype=bool)
+
+    def step_planes(self, x_begin, x_end, side=False):
+        assert 0 <= x_begin < x_end <= self.nx and not self._open[x_begin:x_end].any()
+        self._open[x_begin:x_end] = True
+        self._update(np.arange(x_begin + 1, x_end + 1))
+
+    def step_end(self):
+        assert self._open.all()
+        self._open = None
+        self._advance()
+
+    @property
+    def shape(self):
+        return (self.nx,) + self.fluid.shape[1:]

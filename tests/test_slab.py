@@ -125,7 +125,22 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _gloo_worker(rank, world, port, pattern, steps, seed, outdir):
+@pytest.mark.parametrize("pattern", PATTERNS)
+@pytest.mark.parametrize("dims", [(12, 6, 5), (2, 5, 4), (1, 4, 6)])
+def test_split_step_ring_of_one_matches_periodic_run(pattern, dims):
+    """SlabRunner(overlap=True) on one slab (its own neighbour): interior
+    planes first, then the exchanges and the boundary planes, as the
+    overlapped schedule orders them; slabs of 1 and 2 planes included."""
+    fluid, f0 = _domain(21, dims)
+    ref = M.Periodic(fluid, pattern, f0)
+    ref.run(7)
+    slab = _model_slabs(fluid, f0, pattern, [(0, dims[0])])[0]
+    runner = lbm_slab.SlabRunner(slab, lbm_slab.Ring(), device="cpu", overlap=True)
+    runner.run(7)
+    assert np.array_equal(slab.own_state()[:, fluid], ref.own_state()[:, fluid])
+
+
+def _gloo_worker(rank, world, port, pattern, steps, seed, outdir, overlap=False):
     import torch.distributed as dist
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
                             world_size=world)
@@ -133,7 +148,7 @@ def _gloo_worker(rank, world, port, pattern, steps, seed, outdir):
         fluid, f0 = _domain(seed)
         x0, x1 = lbm_slab.split(fluid.shape[0], world, rank)
         slab = _model_slabs(fluid, f0, pattern, [(x0, x1)])[0]
-        runner = lbm_slab.SlabRunner(slab, lbm_slab.Ring(), device="cpu")
+        runner = lbm_slab.SlabRunner(slab, lbm_slab.Ring(), device="cpu", overlap=overlap)
         runner.run(steps)
         np.save(os.path.join(outdir, f"rank{rank}.npy"), slab.own_state())
         dist.barrier()
@@ -141,13 +156,15 @@ def _gloo_worker(rank, world, port, pattern, steps, seed, outdir):
         dist.destroy_process_group()
 
 
+@pytest.mark.parametrize("overlap", [False, True])
 @pytest.mark.parametrize("pattern", PATTERNS)
 @pytest.mark.parametrize("world", [2, 3])
-def test_slab_runner_over_gloo_matches_periodic_run(pattern, world):
+def test_slab_runner_over_gloo_matches_periodic_run(pattern, world, overlap):
     import torch.multiprocessing as mp
     seed, steps = 11 + world, 6
     with tempfile.TemporaryDirectory() as outdir:
-        mp.start_processes(_gloo_worker, args=(world, _free_port(), pattern, steps, seed, outdir),
+        mp.start_processes(_gloo_worker,
+                           args=(world, _free_port(), pattern, steps, seed, outdir, overlap),
                            nprocs=world, join=True, start_method="spawn")
         got = np.concatenate([np.load(os.path.join(outdir, f"rank{r}.npy"))
                               for r in range(world)], axis=1)

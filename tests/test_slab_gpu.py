@@ -105,6 +105,78 @@ def test_slab_runner_ring_of_one_is_periodic(pattern):
     assert ex == expect
 
 
+@pytest.mark.parametrize("precision", [L.F64, L.F32, L.F16])
+@pytest.mark.parametrize("pattern", PATTERNS)
+@pytest.mark.parametrize("dims", [(18, 12, 10), (9, 6, 128), (2, 8, 64), (1, 9, 7)])
+def test_split_steps_ring_of_one_equal_undecomposed(pattern, precision, dims):
+    """SlabRunner(overlap=True): each step split into the interior planes on
+    the solver's second stream and the boundary planes plus exchanges on its
+    own stream (lbm_step_begin / _planes / _end), bit for bit equal to the
+    undecomposed solver; FP16 at nz = 128 runs the four-cell kernels, slabs
+    of 1 and 2 planes have no interior."""
+    flags, f0 = _domain(dims, 31)
+    ref, _ = _single(flags, f0, pattern, precision, 7)
+    s = _slabs(flags, f0, pattern, precision, 1)[0]
+    runner = lbm_slab.SlabRunner(s, lbm_slab.Ring(), overlap=True)
+    runner.scatter()
+    launches0 = s.launch_count
+    runner.run(7)
+    runner.gather()
+    got = s.get_state()
+    split_launches = s.launch_count - launches0
+    s.close()
+    m = O.fluid_mask(flags)
+    assert np.array_equal(got[:, m], ref[:, m])
+    assert split_launches == 7 * min(dims[0], 3)
+
+
+@pytest.mark.parametrize("pattern", PATTERNS)
+def test_split_steps_on_a_ring_of_three(pattern):
+    flags, f0 = _domain((23, 14, 12), 17)
+    ref, _ = _single(flags, f0, pattern, L.F64, 9)
+    slabs = _slabs(flags, f0, pattern, L.F64, 3)
+    ring = lbm_slab.LocalRing(slabs, overlap=True)
+    ring.scatter()
+    ring.run(9)
+    ring.gather()
+    got = np.concatenate([s.get_state() for s in slabs], axis=1)
+    for s in slabs:
+        s.close()
+    m = O.fluid_mask(flags)
+    assert np.array_equal(got[:, m], ref[:, m])
+
+
+def test_split_step_errors():
+    import torch
+    flags, f0 = _domain((8, 8, 8), 2)
+    buf = torch.empty(1 << 16, dtype=torch.uint8, device="cuda")
+    s = L.Solver.slab(lbm_slab.slab_flags(flags, 0, 8), (0, 0), "push")
+    with pytest.raises(L.LbmError):
+        s.step_planes(0, 8)  # no open step
+    with pytest.raises(L.LbmError):
+        s.step_end()
+    s.step_begin()
+    with pytest.raises(L.LbmError):
+        s.step_begin()  # already open
+    s.step_planes(2, 5, side=True)
+    for bad in ((4, 6), (0, 0), (-1, 1), (7, 9)):
+        with pytest.raises(L.LbmError):
+            s.step_planes(*bad)
+    with pytest.raises(L.LbmError):
+        s.run(1)
+    with pytest.raises(L.LbmError):
+        s.get_state()
+    with pytest.raises(L.LbmError):
+        s.step_end()  # planes 0, 1, 5, 6, 7 missing
+    s.step_planes(0, 2)
+    s.step_planes(5, 8)
+    s.halo_pack(L.HALO_AFTER, buf, buf)  # the open step's messages
+    s.step_end()
+    s.synchronize()
+    assert s.steps_done == 1
+    s.close()
+
+
 @pytest.mark.parametrize("pattern", PATTERNS)
 def test_slab_state_round_trip_in_shifted_orientation(pattern):
     """set_state + scatter, then gather + get_state, return the state, at an
