@@ -71,7 +71,7 @@ struct lbm_solver {
   long long launches;
   size_t dev_bytes;
   int no_shuffle; // reduced precision: never use the shuffle-aligned kernels
-  int no_quad;    // FP16 AA even: never use the four-cell kernel
+  int no_quad;    // FP16 AA: never use the four-cell kernels
   void *u_save_next; // adjoint recomputation: momentum output of the next step
   int slab;          // x-slab of a decomposed domain: device planes 0 and nx+1 are ghosts
   int tma;           // FP64 steps use the bulk-copy pipelined kernels (shape in tma_shape)

@@ -123,7 +123,7 @@ template <class ST> struct StepArgs2 {
   float *u_save;
   Consts2 c;
   int no_shuffle; // host-side switch: use the generic two-cell kernel only
-  int no_quad;    // host-side switch: AA even in FP16 storage on the two-cell kernel
+  int no_quad;    // host-side switch: AA in FP16 storage on the two-cell kernels
   int x0 = 0;     // first storage x plane of the launch (grid.z planes from there)
   int planes = 0; // x planes of the launch
 };
