@@ -100,8 +100,28 @@ __global__ void __launch_bounds__(kStepThreads, (StepOccupancy<ST, KIND>::value)
     return;
   const uint32_t cell = cell_index(g, x, y, z);
   const uint32_t mask = a.mask[cell];
-  if (mask & kSolidBit)
+  if constexpr (kNC) {
+    // Pull and push write a lattice the kernel has not read. A 32-byte
+    // sector of it that holds both fluid and solid cells would be written in
+    // part, and the L2 fetches such a sector from DRAM to merge the write
+    // (14% of the sectors in a 20%-solid porous channel). The solid cells of
+    // those sectors therefore fill their own destination slots, which no
+    // step or transfer reads (a wall's slots hold no population in either
+    // pattern), so the sector is written whole. Lane l holds z = l mod 4 of
+    // its sector: rows start on 32-byte boundaries, blockDim.x % 32 == 0.
+    const unsigned fluid = __ballot_sync(__activemask(), !(mask & kSolidBit));
+    if (mask & kSolidBit) {
+      const int lane = threadIdx.x & 31;
+      if ((fluid >> (lane & ~3)) & 0xFu) {
+#pragma unroll
+        for (int d = 0; d < Q; ++d)
+          a.dst[d * g.plane + cell] = ST::encode(typename ST::V(0), a.c.scale);
+      }
+      return;
+    }
+  } else if (mask & kSolidBit) {
     return;
+  }
   const Offs of = make_offs(g, x, y, z);
   const S *src = a.src;
   S *dst = a.dst;
