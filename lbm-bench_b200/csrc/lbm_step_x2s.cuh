@@ -50,6 +50,29 @@ __global__ void __launch_bounds__(kStepThreads, (PairOccupancy<ST, KIND, true>::
   // directions in which any cell of the warp has a wall link (uniform)
   const uint32_t wlinks = __reduce_or_sync(kFull, (m0 | m1) & 0x7FFFFu);
   const bool links = wlinks != 0u;
+  if (KIND == kPushStep) {
+    // Push writes a lattice this kernel has not read, and only the fluid
+    // cells' targets: a 32-byte sector holding solid cells too would be
+    // written in part and fetched from DRAM by the L2 to merge the write.
+    // The solid cells of sectors that hold fluid fill their own slots
+    // (d, x), which nothing reads (a bounced population may land there too,
+    // an equally unread value), so the sector is written whole.
+    constexpr int kSectorLanes = 16 / (int)sizeof(S); // two cells per lane
+    const unsigned lanes = __ballot_sync(kFull, fluid0 || fluid1);
+    const unsigned group = (lanes >> (lane & ~(kSectorLanes - 1))) & ((1u << kSectorLanes) - 1u);
+    if (group && !(fluid0 && fluid1)) {
+#pragma unroll
+      for (int d = 0; d < Q; ++d) {
+        S *own = a.dst + d * g.plane + cell;
+        if (!fluid0 && !fluid1)
+          *reinterpret_cast<P *>(own) = PT::enc(f2(0.f));
+        else if (!fluid0)
+          own[0] = PT::enc1(0.f);
+        else
+          own[1] = PT::enc1(0.f);
+      }
+    }
+  }
 
   // x/y parts of the neighbour offsets (uniform across the warp); the z
   // shift is handled by shuffles and the two edge lanes
