@@ -56,8 +56,23 @@ __global__ void __launch_bounds__(128, LBM_MINB_ADJ) adjoint_step_kernel(AdjArgs
     return;
   const uint32_t cell = cell_index(g, x, y, z);
   const uint32_t mask = a.mask[cell];
-  if (mask & kSolidBit)
+  // The step writes lambda into a lattice it has not read. The solid cells
+  // of 32-byte sectors that also hold fluid cells store their own lambda
+  // (0, as the seed sets it; no step reads a wall's slots), so that such
+  // sectors are written whole and the L2 does not fetch them from DRAM to
+  // merge a partial write. Lane l holds z = l mod (32 / sizeof(V)) of its
+  // sector: rows start on 32-byte boundaries and blockDim.x % 32 == 0.
+  const unsigned fluid = __ballot_sync(__activemask(), !(mask & kSolidBit));
+  if (mask & kSolidBit) {
+    constexpr int kSectorLanes = 32 / (int)sizeof(V);
+    const int lane = threadIdx.x & 31;
+    if ((fluid >> (lane & ~(kSectorLanes - 1))) & ((1u << kSectorLanes) - 1u)) {
+#pragma unroll
+      for (int k = 0; k < Q; ++k)
+        a.lam[k * g.plane + cell] = V(0);
+    }
     return;
+  }
   const Offs of = make_offs(g, x, y, z);
   const long long P = g.plane;
 
