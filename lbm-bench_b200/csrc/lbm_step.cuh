@@ -2,7 +2,9 @@
 //
 // One thread per lattice cell, z (the unit-stride axis) across the lanes of
 // a warp, so every population plane is read and written in 32-wide
-// contiguous runs. Wall cells return after reading their mask word.
+// contiguous runs. Wall cells return after reading their mask word (in pull
+// and push, those that share a 32-byte sector with fluid cells first fill
+// their own destination slots, see step_kernel).
 //
 // The reference runs a dense sweep and then a serial bounce-back list pass
 // (src/kernel_pull_soa.c:94-204, src/kernel_push_soa.c:94-204,
@@ -15,22 +17,23 @@
 //            read f_d(x)                         write out_d
 //   pull     back(d) ? src[inv d][x]             dst[d][x], + F_inv d if bb(d) else + F_d
 //                    : src[d][x - c_d]
-//   push     src[d][x]                           dst[d][x + c_d] + F_d; if bb(d) also
-//                                                dst[inv d][x] = out_d + F_inv d
+//   push     src[d][x]                           bb(d) ? dst[inv d][x] = out_d + F_inv d
+//                                                      : dst[d][x + c_d] = out_d + F_d
 //   AA even  A[d][x]                             A[inv d][x], + F_inv d if bb(d) else + F_d
-//   AA odd   back(d) ? A[d][x]                   A[d][x + c_d] + F_d; if bb(d) also
-//                    : A[inv d][x - c_d]         A[inv d][x] = out_d + F_inv d
+//   AA odd   back(d) ? A[d][x]                   bb(d) ? A[inv d][x] = out_d + F_inv d
+//                    : A[inv d][x - c_d]               : A[d][x + c_d] = out_d + F_d
 //
-// In push and AA odd the first store of a bounced population lands in the
-// wall cell's slot, which nothing reads; this keeps that store free of a
-// per-lane address choice. Every stored value is fl(out_d + F), the single
+// (With LBM_STORE_MIRROR, measured slower, push and AA odd store every
+// population to [d][x + c_d], a bounced one into the wall cell's unread
+// slot, and the bounced value again into [inv d][x].) Every stored value is
+// fl(out_d + F), the single
 // rounding the reference performs when kernelAddBodyForce
 // (src/lbm.c:902-922) adds the force to the populations a fluid cell
 // receives, so the FP64 kernels are bit-identical to the reference's.
 // Race freedom of the in-place AA odd step: a cell reads
 // {(e, x + c_e) : x + c_e fluid} and {(d, x) : back(d)}, and writes the same
-// sets plus wall slots; the sets of different cells are disjoint and wall
-// cells never run.
+// sets; the sets of different cells are disjoint and wall cells do not
+// update.
 #pragma once
 
 #include "lbm_device.cuh"
@@ -60,19 +63,24 @@ template <class ST> struct StepArgs {
 #ifndef LBM_MINB_LP
 #define LBM_MINB_LP 4
 #endif
-// Per kind for FP64, from a sweep on the 256^3 porous channel (B200): the
-// AA odd step is fastest at 7 CTAs per SM (72 registers), pull at 5 (96),
-// AA even and push at 6 (80); 8 spills.
+// Per kind for FP64, from sweeps on the 256^3 porous channel (B200): the
+// AA odd step is fastest at 7 CTAs per SM (72 registers), AA even at 6
+// (80); with the partial-sector fill, pull at 6 (80) and push at 5 (96).
+// 8 spills.
 #ifndef LBM_MINB_F64_ODD
 #define LBM_MINB_F64_ODD 7
 #endif
 #ifndef LBM_MINB_F64_PULL
-#define LBM_MINB_F64_PULL 5
+#define LBM_MINB_F64_PULL 6
+#endif
+#ifndef LBM_MINB_F64_PUSH
+#define LBM_MINB_F64_PUSH 5
 #endif
 template <class ST, int KIND> struct StepOccupancy {
   static constexpr int value = sizeof(typename ST::S) != 8 ? LBM_MINB_LP
       : KIND == kAAOddStep ? LBM_MINB_F64_ODD
-      : KIND == kPullStep ? LBM_MINB_F64_PULL : LBM_MINB_F64;
+      : KIND == kPullStep ? LBM_MINB_F64_PULL
+      : KIND == kPushStep ? LBM_MINB_F64_PUSH : LBM_MINB_F64;
 };
 
 // Read-only loads of the two-lattice patterns may take the non-coherent
