@@ -714,6 +714,16 @@ def run_reference(args):
     }
 
 
+def _json_channel():
+    """The one JSON line goes to the process's standard output; everything
+    else written to file descriptor 1 - the C libraries' progress lines, the
+    reference's printf, NCCL - is sent to standard error instead."""
+    sys.stdout.flush()
+    out = os.fdopen(os.dup(1), "w")
+    os.dup2(2, 1)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -731,6 +741,12 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    out = _json_channel()
+
+    def emit(obj):
+        out.write(json.dumps(obj) + "\n")
+        out.flush()
+
     if args.config != 1:
         if args.impl == "reference" or args.gpus != 1:
             ap.error("--config 2-4 run the native arm on one GPU")
@@ -740,18 +756,18 @@ def main():
         if "--size" not in sys.argv:
             args.size = None
         fn = {2: run_precision_study, 3: run_adjoint_only, 4: run_largest}[args.config]
-        print(json.dumps(fn(args)), flush=True)
+        emit(fn(args))
         return
     if args.impl == "reference":
         res = run_reference(args)
         if res is not None:
-            print(json.dumps(res), flush=True)
+            emit(res)
         return
     dist = Dist(args.gpus)
     try:
         res = run_native(args, dist)
         if dist.rank == 0:
-            print(json.dumps(res), flush=True)
+            emit(res)
     finally:
         dist.close()
 
