@@ -35,14 +35,16 @@ static cudaError_t go(const StepArgs2<ST> &a, dim3 grid, dim3 block, cudaStream_
       }
     }
   }
-  if (KIND != kAAEvenStep && a.g.nz % 64 == 0 && !a.no_shuffle) {
-    dim3 sg, sb;
-    shuffle_launch_shape(a.g, sg, sb);
-    sg.z = a.planes;
-    step_kernel_x2s<ST, KIND, FORCE, BRINK><<<sg, sb, 0, st>>>(a);
-  } else {
-    step_kernel_x2<ST, KIND, FORCE, BRINK><<<grid, block, 0, st>>>(a);
+  if constexpr (KIND != kAAEvenStep) { // AA even is local: nothing to realign
+    if (a.g.nz % 64 == 0 && !a.no_shuffle) {
+      dim3 sg, sb;
+      shuffle_launch_shape(a.g, sg, sb);
+      sg.z = a.planes;
+      step_kernel_x2s<ST, KIND, FORCE, BRINK><<<sg, sb, 0, st>>>(a);
+      return cudaGetLastError();
+    }
   }
+  step_kernel_x2<ST, KIND, FORCE, BRINK><<<grid, block, 0, st>>>(a);
   return cudaGetLastError();
 }
 
