@@ -196,9 +196,15 @@ class Dist:
 # CPU baseline: LBM-Bench's own kernels (oracle/_ref)
 # ---------------------------------------------------------------------------
 
+MARCH = {"bench_v4": "x86-64-v4", "bench_v3": "x86-64-v3"}
+
+
 def reference_cpu(flags, f0, budget_s: float, max_steps: int, kernels=("push-soa", "pull-soa")):
-    """Times the reference's OpenMP kernels on this host on the workload.
-    Returns dict(value MLUPS, kernel, steps, cores, variant) or raises."""
+    """Times the reference's OpenMP kernels on this host on the workload:
+    both OpenMP kernels are calibrated on 2 steps, the faster one is timed
+    on as many steps as fit in `budget_s` (at most max_steps). Returns
+    dict(value MLUPS, kernel, steps, cores, variant, seconds, sample) or
+    raises FileNotFoundError when the reference build is missing."""
     ncores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(ncores))
     os.environ.setdefault("OMP_PROC_BIND", "close")
@@ -220,8 +226,13 @@ def reference_cpu(flags, f0, budget_s: float, max_steps: int, kernels=("push-soa
     k, d2 = best
     steps = max(2, min(max_steps, int(budget_s / max(d2 / 2, 1e-6))))
     _, dur, _, _ = ref.run(k, flags, per, f0, steps, 1.25, 1e-6, readback=False)
+    nz, ny, nx = flags.shape
+    sample = (f"{k}, LBM-Bench's own OpenMP kernel (faster of push-soa/pull-soa on a 2-step "
+              f"calibration), built -O3 -ffast-math -fopenmp -march={MARCH[variant]}, "
+              f"{threads} threads, {steps} steps of the {nx}x{ny}x{nz} porous channel, "
+              f"{dur:.1f} s")
     return {"value": n_fluid * steps / dur / 1e6, "kernel": k, "steps": steps, "cores": threads,
-            "variant": variant, "seconds": dur}
+            "variant": variant, "seconds": dur, "sample": sample}
 
 
 def _has_avx512() -> bool:
@@ -240,6 +251,16 @@ def make_workload(L, n: int):
     flags, frac, nsph = L.porous_channel((n, n, n), 0.2, 4.0, 8.0, seed=42)
     f0 = L.perturbed_equilibrium(flags, seed=7, amplitude=1e-4)
     return flags, f0, frac, nsph
+
+
+def workload_config(n, frac, nsph, n_fluid):
+    """The `config` both arms print for the n^3 porous-channel workload."""
+    cfg = dict(WORKLOAD, solid_fraction_achieved=frac, spheres=nsph, fluid_cells=n_fluid,
+               parallelism="single process")
+    if n != 256:
+        cfg.update(workload=f"porous channel {n}^3, 20% solid spheres r 4-8, seed 42",
+                   dims=[n, n, n])
+    return cfg
 
 
 def solver(L, flags, pattern, precision, f0):
@@ -333,8 +354,7 @@ def run_native(args, dist: Dist):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded porous geometry and initial state)",
-        "config": dict(WORKLOAD, solid_fraction_achieved=frac, spheres=nsph,
-                       fluid_cells=n_fluid, parallelism=f"replicas x{dist.world}"),
+        "config": workload_config(n, frac, nsph, n_fluid),
         "gbs": n_fluid * bpu * args.steps / (ms / 1e3) / 1e9,
         "roofline": roofline, "e2e": e2e, "gpu_launches": launches,
         "clocks": clk.summary(), "variants": variants, "adjoint": adjoint,
@@ -347,8 +367,7 @@ def run_native(args, dist: Dist):
             cb = reference_cpu(flags, f0, budget_s=args.cpu_seconds, max_steps=args.steps)
             result["cpu_baseline"] = {
                 "value": cb["value"], "unit": "MLUPS", "cores": cb["cores"], "kind": "reference",
-                "sample": f"{cb['kernel']} (OpenMP, {cb['variant']}) on the same 256^3 porous "
-                          f"channel, {cb['steps']} steps, {cb['seconds']:.1f} s"}
+                "sample": cb["sample"]}
         except Exception as exc:  # reported, not fatal
             result["cpu_baseline"] = {"value": None, "unit": "MLUPS", "error": str(exc)}
     return result
@@ -685,12 +704,18 @@ def run_e2e(L, flags, f0, steps, dist: Dist):
 
 
 def run_reference(args):
-    """LBM-Bench's own CPU kernels on this host, same workload and metric."""
-    import lbmb200 as L
+    """LBM-Bench's own CPU kernels on this host, same workload, metric and
+    config as the native arm. Nothing of the product is loaded: the inputs
+    come from the oracle's restatement of the workload generator (checked
+    bit for bit against the product's in tests/test_host.py)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
-    flags, f0, frac, nsph = make_workload(L, args.size)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    n = args.size
+    flags, frac, nsph = O.porous_channel((n, n, n), 0.2, 4.0, 8.0, seed=42)
+    f0 = O.counter_equilibrium(flags, 7, 1e-4)
     try:
         cb = reference_cpu(flags, f0, budget_s=args.cpu_seconds * 3, max_steps=args.steps)
     except FileNotFoundError as exc:
@@ -703,12 +728,10 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": cb["seconds"] * 1e3 / cb["steps"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded porous geometry and initial state)",
-        "config": dict(WORKLOAD, solid_fraction_achieved=frac, spheres=nsph,
-                       fluid_cells=n_fluid, parallelism="host CPU (OpenMP)"),
+        "config": workload_config(n, frac, nsph, n_fluid),
+        "execution": f"host CPU, {cb['cores']} OpenMP threads",
         "cpu_baseline": {"value": value, "unit": "MLUPS", "cores": cb["cores"],
-                         "kind": "reference",
-                         "sample": f"{cb['kernel']} ({cb['variant']}), {cb['steps']} steps of "
-                                   "the 256^3 workload"},
+                         "kind": "reference", "sample": cb["sample"]},
         "e2e": {"value": value, "unit": "MLUPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }

@@ -224,23 +224,35 @@ int lbm_mass_momentum(lbm_solver *s, double out[4], long long *nonfinite);
 
 /* No counterpart in the reference. Same totals as lbm_mass_momentum, for a
  * caller that holds the populations itself and must not allocate device
- * memory: code running while a CUDA graph is captured (cudaMalloc is refused
- * then), plug-ins whose host application's allocator owns the device memory,
- * and loops that cannot afford cudaMalloc's device-wide synchronisation.
- * This call allocates nothing: its scratch is a fixed array inside the
- * library that every GPU loading the library holds until exit.
+ * memory: a plug-in inside a host application whose own caching allocator
+ * already owns the GPU's memory (a cudaMalloc from the plug-in can fail or
+ * fragment the pool behind the application's back), and control loops that
+ * cannot afford the device-wide synchronisation cudaMalloc and cudaFree may
+ * imply. This call allocates nothing: its scratch is a fixed array inside
+ * the library that every GPU loading the library holds until exit
+ * ((LBM_NOALLOC_MAX_PLANES + 1) rows of 6 doubles, 384 KiB).
  *   f      device pointer, double[19*nx*ny*nz] in the f[d][x][y][z] layout
  *   flags  device pointer, int[nx*ny*nz] in latticeIndex order, 0 = obstacle
  *   out    host double[4]: mass, momentum x, y, z over fluid cells (FP64)
  *   nonfinite  host, may be NULL: fluid cells holding NaN/Inf (if non-zero
  *          the call returns LBM_ERR_NONFINITE after filling out)
- *   stream cudaStream_t as void* (NULL = default stream); the call waits
- *          for its own work on that stream.
+ *   stream cudaStream_t as void* (NULL = default stream). The call is
+ *          synchronous: it copies the totals to the host and waits on that
+ *          stream (cudaStreamSynchronize) before it returns.
+ * f and flags must live on the device that is current at the call (the
+ * scratch address is looked up for that device); a pointer on another
+ * device is rejected with LBM_ERR_ARG.
  * Limit: nx <= LBM_NOALLOC_MAX_PLANES (one scratch row per x-plane); larger
- * boxes are rejected with LBM_ERR_ARG. The first call on each device looks
- * up the scratch's device address; make it before any stream capture.
- * Calls share the scratch: calls whose work overlaps on the GPU race, so
- * serialise them. */
+ * boxes are rejected with LBM_ERR_ARG. One block sums each x-plane, so a
+ * box with few x-planes (e.g. 8 x 1024 x 1024) runs on few SMs and takes
+ * longer than lbm_mass_momentum; flags are read with a stride of nx ints
+ * between neighbouring threads.
+ * The first call on each device looks up the scratch's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture is started on the device.
+ * Calls share the scratch: every row a call reads it has written first, but
+ * calls whose work overlaps on the GPU (two streams, two host threads) race
+ * on the rows, so serialise them. */
 #define LBM_NOALLOC_MAX_PLANES 8192
 int lbm_mass_momentum_noalloc(const double *f, const int *flags, int nx, int ny, int nz,
     double out[4], long long *nonfinite, void *stream);

@@ -1,12 +1,12 @@
 // lbm_mass_momentum_noalloc: the FP64 mass/momentum/NaN reduction of
 // lbm_mass_momentum, for callers that must not allocate device memory.
 //
-// Who cannot allocate: code that runs while a CUDA graph is being captured
-// (cudaMalloc is refused during a global-mode capture), plug-ins inside a
-// host application whose caching allocator already holds the device's
-// memory, and tight control loops where cudaMalloc's implicit device-wide
-// synchronisation is not acceptable. Such a caller owns the population and
-// flag buffers and only wants the diagnostic.
+// Who cannot allocate: a plug-in inside a host application whose caching
+// allocator already holds the device's memory (a cudaMalloc behind its back
+// can fail or fragment that pool), and control loops where the device-wide
+// synchronisation that cudaMalloc/cudaFree may imply is not acceptable. Such
+// a caller owns the population and flag buffers and only wants the
+// diagnostic.
 //
 // The reduction needs scratch for its per-block partial sums. Here that
 // scratch is a file-scope device array of fixed size: one row per x-plane,
@@ -15,13 +15,14 @@
 // about 384 KiB) until the process exits. All calls share it; a call writes
 // every row it later reads, so no clearing is needed, but two calls whose
 // kernels overlap on the GPU race on the rows - serialise them (one stream,
-// or synchronise in between).
+// or synchronise in between). The call itself is synchronous: it copies the
+// totals to the host and synchronises the caller's stream.
 //
 // Host code cannot use the array's name as a device address (in host code
 // it names a host-side stand-in). The device address is looked up once per
 // device, with that device current, through cudaGetSymbolAddress on the
-// first call made on that device; make that first call before starting any
-// stream capture.
+// first call made on that device; make that first call before any stream
+// capture is started on the device.
 #include <mutex>
 
 #include "lbm_b200.h"
@@ -127,6 +128,29 @@ int rows_on_current_device(double **out)
   return LBM_OK;
 }
 
+// LBM_OK if p is device memory of the current device (or managed memory).
+int on_current_device(const void *p, const char *name)
+{
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  cudaPointerAttributes a {};
+  if (e == cudaSuccess)
+    e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return record_error(LBM_ERR_ARG, "lbm_mass_momentum_noalloc: %s is not a device pointer (%s)",
+        name, cudaGetErrorString(e));
+  }
+  if (a.type == cudaMemoryTypeManaged)
+    return LBM_OK;
+  if (a.type != cudaMemoryTypeDevice || a.device != dev)
+    return record_error(LBM_ERR_ARG,
+        "lbm_mass_momentum_noalloc: %s must be device memory of the current device %d "
+        "(memory type %d, device %d)",
+        name, dev, (int)a.type, a.device);
+  return LBM_OK;
+}
+
 } // namespace
 
 extern "C" int lbm_mass_momentum_noalloc(const double *f, const int *flags, int nx, int ny,
@@ -141,6 +165,11 @@ extern "C" int lbm_mass_momentum_noalloc(const double *f, const int *flags, int 
         nx, kMaxPlanes);
   double *rows = nullptr;
   int rc = rows_on_current_device(&rows);
+  if (rc)
+    return rc;
+  rc = on_current_device(f, "f");
+  if (!rc)
+    rc = on_current_device(flags, "flags");
   if (rc)
     return rc;
   cudaStream_t st = (cudaStream_t)stream;

@@ -289,3 +289,111 @@ def moments(f, flags):
     uz = np.tensordot(CZ.astype(np.float64), f, axes=(0, 0))
     m = fluid_mask(flags)
     return [np.where(m, a, 0.0) for a in (rho, ux, uy, uz)]
+
+
+# ---------------------------------------------------------------------------
+# The benchmark workload, restated without the product library: the seeded
+# porous channel and the counter-based perturbed equilibrium. The reference
+# has no sphere generator or seeded initial state of its own; these are the
+# inputs the benchmark feeds to both arms, so the reference arm builds them
+# here and a CPU test checks them bit for bit against the product's C
+# generator (lbm_porous_channel / lbm_perturbed_equilibrium).
+# ---------------------------------------------------------------------------
+
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+def _mix64(z):
+    """splitmix64 finaliser (Steele, Lea, Flood 2014), wrapping uint64."""
+    z = (z ^ (z >> np.uint64(30))) * _M1
+    z = (z ^ (z >> np.uint64(27))) * _M2
+    return z ^ (z >> np.uint64(31))
+
+
+def _u01(v):
+    """Uniform double in [0, 1) from the top 53 bits."""
+    return (v >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def channel(dims):
+    """The reference's `channel` geometry (src/lbm.c:52-187 with x forced
+    periodic, src/lbm.c:96-102): obstacle cells at y, z in {0, n-1}.
+    Returns int32[nz, ny, nx] flags."""
+    nx, ny, nz = dims
+    flags = np.ones((nz, ny, nx), dtype=np.int32)
+    flags[:, [0, ny - 1], :] = 0
+    flags[[0, nz - 1], :, :] = 0
+    return flags
+
+
+def porous_channel(dims, solid_fraction=0.2, rmin=4.0, rmax=8.0, seed=42):
+    """Channel plus seeded solid spheres until the solid fraction (walls
+    included) reaches `solid_fraction`: per sphere four splitmix64 draws
+    (centre x, y, z uniform over the box, radius uniform in [rmin, rmax]);
+    a cell is solid when its squared distance to the centre is <= r^2, with
+    x wrapped periodically. Returns (flags, fraction, n_spheres)."""
+    nx, ny, nz = dims
+    flags = channel(dims)
+    total = nx * ny * nz
+    solid = int((flags == 0).sum())
+    state = np.uint64(seed)
+    spheres = 0
+    with np.errstate(over="ignore"):
+        while solid < solid_fraction * total:
+            draws = []
+            for _ in range(4):
+                state = state + _GOLDEN
+                draws.append(float(_u01(_mix64(np.array([state], dtype=np.uint64)))[0]))
+            cxs, cys, czs = draws[0] * nx, draws[1] * ny, draws[2] * nz
+            r = rmin + (rmax - rmin) * draws[3]
+            ir = int(np.ceil(r))
+            r2 = r * r
+            d = np.arange(-ir - 1, ir + 2)
+            zs = int(np.floor(czs)) + d
+            ys = int(np.floor(cys)) + d
+            xs = int(np.floor(cxs)) + d
+            zs = zs[(zs >= 0) & (zs < nz)]
+            ys = ys[(ys >= 0) & (ys < ny)]
+            ez = (zs - czs)[:, None, None]
+            ey = (ys - cys)[None, :, None]
+            ex = (xs - cxs)[None, None, :]
+            inside = (ex * ex + ey * ey) + ez * ez <= r2
+            xw = xs % nx
+            zi, yi, xi = np.nonzero(inside)
+            sel = (zs[zi], ys[yi], xw[xi])
+            hit = flags[sel] != 0
+            flags[sel] = 0
+            # a wrapped x can repeat within one sphere only if 2 ir + 3 > nx
+            solid += int(np.unique(np.stack(sel)[:, hit], axis=1).shape[1]) \
+                if 2 * ir + 3 > nx else int(hit.sum())
+            spheres += 1
+    return flags, solid / total, spheres
+
+
+def counter_equilibrium(flags, seed, amplitude=1e-4, rho=1.0):
+    """Equilibrium at density rho with a velocity perturbation drawn per
+    fluid cell from a counter-based splitmix64 stream: cell c (f's cell
+    order, z fastest) starts from seed ^ mix64(c * golden + 1) and takes
+    three draws, u_k = amplitude (2 U - 1). Obstacle entries are 0.
+    Returns float64[19, nx, ny, nz]."""
+    nz, ny, nx = flags.shape
+    n = nx * ny * nz
+    c = np.arange(n, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        base = np.uint64(seed) ^ _mix64(c * _GOLDEN + np.uint64(1))
+        u = []
+        for _ in range(3):
+            base = base + _GOLDEN
+            u.append(amplitude * (2.0 * _u01(_mix64(base)) - 1.0))
+    del base, c
+    ux, uy, uz = (a.reshape(nx, ny, nz) for a in u)
+    usq = ux * ux + uy * uy + uz * uz
+    fluid = fluid_mask(flags)
+    f = np.empty((Q, nx, ny, nz))
+    for d in range(Q):
+        cu = float(CX[d]) * ux + float(CY[d]) * uy + float(CZ[d]) * uz
+        f[d] = W[d] * (((rho - 1.5 * usq) + 3.0 * cu) + 4.5 * cu * cu)
+        f[d][~fluid] = 0.0
+    return f

@@ -45,6 +45,34 @@ def test_reference_arm_prints_the_contract_line():
                         "d2h_bytes_per_step": 0}
 
 
+@pytest.mark.skipif(not (O.ref_available("bench_v3") or O.ref_available("bench_v4")),
+                    reason="oracle/_ref not built here")
+def test_reference_arm_loads_nothing_from_the_product():
+    """The reference arm builds its workload with the oracle's generator:
+    neither the lbmb200 module nor liblbmb200.so may be loaded in it."""
+    code = (
+        "import atexit, runpy, sys\n"
+        "def check():\n"
+        "    maps = open('/proc/self/maps').read()\n"
+        "    sys.stderr.write('\\nPRODUCT_LOADED\\n' if ('liblbmb200' in maps or\n"
+        "                     'lbmb200' in sys.modules) else '\\nPRODUCT_ABSENT\\n')\n"
+        "atexit.register(check)\n"
+        f"sys.argv = [{BENCH!r}, '--impl', 'reference', '--steps', '2', '--warmup', '3',\n"
+        "            '--size', '40', '--cpu-seconds', '1']\n"
+        f"runpy.run_path({BENCH!r}, run_name='__main__')\n")
+    e = dict(os.environ)
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
+        e.pop(k, None)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       timeout=300, env=e, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "PRODUCT_ABSENT" in r.stderr and "PRODUCT_LOADED" not in r.stderr
+    d = json.loads([ln for ln in r.stdout.splitlines() if ln.strip()][0])
+    assert d["impl"] == "reference" and d["value"] > 0
+    assert d["config"]["dims"] == [40, 40, 40]
+    assert "-march=x86-64-v" in d["cpu_baseline"]["sample"]
+
+
 def test_reference_arm_runs_on_rank_0_only():
     r = _run("--impl", "reference", "--steps", "1", "--warmup", "3",
              env={"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}, timeout=120)

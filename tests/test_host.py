@@ -112,3 +112,20 @@ def test_product_path_fails_loudly_without_gpu():
         L.Solver(flags, per)
     assert e.value.code == -6
     assert "no CPU path" in str(e.value)
+
+
+@pytest.mark.parametrize("dims,frac,rmin,rmax,seed", [
+    ((40, 36, 44), 0.2, 4.0, 8.0, 42), ((64, 48, 32), 0.3, 6.0, 12.0, 5),
+    ((8, 30, 26), 0.25, 4.0, 8.0, 3),  # 2r + 3 > nx: one sphere wraps onto itself in x
+    ((17, 19, 23), 0.0, 4.0, 8.0, 1)])
+def test_oracle_workload_equals_product_generator(dims, frac, rmin, rmax, seed):
+    """The benchmark's reference arm builds its inputs with the oracle's
+    numpy restatement; it must be bit-identical to the product's C
+    generator so both arms run the same workload."""
+    flags, f_frac, n_sph = L.porous_channel(dims, frac, rmin, rmax, seed=seed)
+    oflags, o_frac, o_sph = O.porous_channel(dims, frac, rmin, rmax, seed=seed)
+    assert np.array_equal(flags, oflags)
+    assert (f_frac, n_sph) == (o_frac, o_sph)
+    f = L.perturbed_equilibrium(flags, seed=7, amplitude=1e-4)
+    fo = O.counter_equilibrium(oflags, 7, 1e-4)
+    assert f.tobytes() == fo.tobytes()

@@ -39,14 +39,21 @@ def _state(kind, dims, steps, seed):
     return flags, f, totals, bad
 
 
-def _noalloc(f_dev, flags_dev, dims):
+def _noalloc(f_dev, flags_dev, dims, stream=None):
     nx, ny, nz = dims
     out = np.zeros(4)
     bad = ctypes.c_longlong(-1)
+    handle = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
     rc = L.lib().lbm_mass_momentum_noalloc(
         ctypes.c_void_p(f_dev.data_ptr()), ctypes.c_void_p(flags_dev.data_ptr()), nx, ny, nz,
-        out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(bad), None)
+        out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(bad), handle)
     return rc, out, bad.value
+
+
+def _check(out, ref, kind):
+    assert out[0] == pytest.approx(ref[0], rel=MASS_REL)
+    for k in (1, 2, 3):
+        assert out[k] == pytest.approx(ref[k], rel=MOMENTUM_REL, abs=MOMENTUM_ABS), (kind, k)
 
 
 def test_noalloc_reduction_matches_solver_on_two_calls_in_a_row():
@@ -60,9 +67,47 @@ def test_noalloc_reduction_matches_solver_on_two_calls_in_a_row():
         rc, out, bad = _noalloc(f_dev, flags_dev, dims)
         assert rc == 0, L.lib().lbm_last_error()
         assert bad == 0 and ref_bad == 0
-        assert out[0] == pytest.approx(ref[0], rel=MASS_REL)
-        for k in (1, 2, 3):
-            assert out[k] == pytest.approx(ref[k], rel=MOMENTUM_REL, abs=MOMENTUM_ABS), (kind, k)
+        _check(out, ref, kind)
+
+
+def test_noalloc_on_caller_stream_and_nonfinite_count():
+    """A caller-owned stream, queued behind the caller's own work on it;
+    then two fluid cells poisoned with NaN and Inf: the call fills the
+    totals, counts both cells and returns LBM_ERR_NONFINITE (-4)."""
+    torch = pytest.importorskip("torch")
+    dims = (40, 24, 28)
+    flags, f, ref, _ = _state("porous", dims, 5, 9)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        f_dev = torch.from_numpy(np.ascontiguousarray(f)).to("cuda", non_blocking=False)
+        flags_dev = torch.from_numpy(np.ascontiguousarray(flags)).to("cuda")
+        scaled = f_dev * 1.0  # work queued on the caller's stream before the call
+    rc, out, bad = _noalloc(scaled, flags_dev, dims, stream)
+    assert rc == 0, L.lib().lbm_last_error()
+    assert bad == 0
+    _check(out, ref, "stream")
+    fluid = np.argwhere(np.transpose(flags, (2, 1, 0)) != 0)
+    (x0, y0, z0), (x1, y1, z1) = fluid[0], fluid[len(fluid) // 2]
+    poisoned = scaled.clone()
+    poisoned[3, x0, y0, z0] = float("nan")
+    poisoned[18, x1, y1, z1] = float("inf")
+    torch.cuda.synchronize()
+    rc, out, bad = _noalloc(poisoned, flags_dev, dims, stream)
+    assert rc == -4  # LBM_ERR_NONFINITE
+    assert bad == 2
+    assert b"2 fluid cells" in L.lib().lbm_last_error()
+
+
+def test_noalloc_rejects_host_pointer():
+    """f must be device memory of the current device."""
+    torch = pytest.importorskip("torch")
+    dims = (4, 4, 4)
+    f_host = torch.zeros((19,) + dims, dtype=torch.float64)
+    flags_dev = torch.ones(dims, dtype=torch.int32, device="cuda")
+    rc, _, _ = _noalloc(f_host, flags_dev, dims)
+    assert rc == -1
+    assert b"must be device memory" in L.lib().lbm_last_error() or \
+        b"not a device pointer" in L.lib().lbm_last_error()
 
 
 def test_noalloc_rejects_box_beyond_scratch():
