@@ -362,6 +362,11 @@ def run_native(args, dist: Dist):
         "device_bytes": s.device_bytes,
     }
     s.close()
+    if not args.no_studies:
+        result["precision_512"] = precision_study(L, 512, 300, peak)
+        result["largest"] = largest_study(L, 768, 200, peak)
+    if not args.no_parity:
+        result["parity"] = parity_study(L, flags, f0)
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         try:
             cb = reference_cpu(flags, f0, budget_s=args.cpu_seconds, max_steps=args.steps)
@@ -370,7 +375,129 @@ def run_native(args, dist: Dist):
                 "sample": cb["sample"]}
         except Exception as exc:  # reported, not fatal
             result["cpu_baseline"] = {"value": None, "unit": "MLUPS", "error": str(exc)}
+    result["summary"] = summary(result)
     return result
+
+
+def _r(v, digits=4):
+    """v rounded to `digits` significant digits (None stays None)."""
+    if v is None:
+        return None
+    if isinstance(v, bool) or not isinstance(v, (int, float)):
+        return v
+    return float(f"{v:.{digits}g}")
+
+
+def summary(r):
+    """The headline figures of the default line in one short object, placed
+    last so that a reader of only the line's tail still sees them: MLUPS and
+    roofline fraction per precision and pattern, errors against FP64, the
+    adjoint's cost, and the parity of configs 0 and 1 with the reference."""
+    v = r.get("variants", {})
+    out = {"fp64_aa": {"mlups": _r(r["value"]), "frac_step": _r(r["gbs"] / r["roofline"]["peak"]),
+                       "frac_odd": _r(r["roofline"]["frac"])}}
+    for k in ("fp64_pull", "fp64_push"):
+        if k in v:
+            out[k] = {"mlups": _r(v[k]["mlups"]), "frac": _r(v[k]["frac"])}
+    for k in ("fp32_aa", "fp32_pull", "fp16_aa", "fp16_pull"):
+        if k in v and v[k]["mlups"]:
+            out[k] = {"mlups": _r(v[k]["mlups"]), "frac": _r(v[k]["frac"]),
+                      "x_fp64_aa": _r(v[k]["speedup_vs_fp64_aa"], 3),
+                      "err_u": _r(v[k]["l2_rel_err_u"], 2), "err_rho": _r(v[k]["l2_rel_err_rho"], 2)}
+    p = r.get("precision_512")
+    if p:
+        out["p512"] = {"fp64_aa": _r(p["fp64_aa"]["mlups"])}
+        for k in ("fp32_aa", "fp16_aa"):
+            out["p512"][k] = {"mlups": _r(p[k]["mlups"]), "frac": _r(p[k]["frac"]),
+                              "x_fp64_aa": _r(p[k]["speedup_vs_fp64_aa"], 3),
+                              "err_u": _r(p[k]["l2_rel_err_u"], 2),
+                              "err_rho": _r(p[k]["l2_rel_err_rho"], 2)}
+    g = r.get("largest")
+    if g:
+        f = g["forward_fp16_aa"]
+        a = g["adjoint"]["fp32"]
+        out["l768_fp16_aa"] = {"mlups": _r(f["mlups"]), "frac": _r(f["frac"]),
+                               "device_gb": _r(f["device_used_bytes"] / 1e9, 3)}
+        out["adj384_fp32"] = {"cost_fwd_steps": _r(a["cost_in_forward_steps"], 3),
+                              "s_per_step": _r(a["s_per_step"], 3),
+                              "peak_gb": _r(a["peak_device_bytes"] / 1e9, 3)}
+    a = r.get("adjoint")
+    if a:
+        out["adj128"] = {"fp64_cost": _r(a["fp64"]["cost_in_forward_steps"], 3),
+                         "fp32_cost": _r(a["fp32"]["cost_in_forward_steps"], 3),
+                         "interval": a["fp64"]["checkpoint_interval"]}
+        if "fp64_auto_schedule" in a:
+            out["adj128"]["fp64_auto_cost"] = _r(a["fp64_auto_schedule"]["cost_in_forward_steps"], 3)
+        if "fd_check" in a:
+            fd = a["fd_check"]
+            out["adj128"]["fd_eps1e-4_max_rel"] = _r(fd["eps_0.0001"]["max_rel_err"], 3)
+            out["adj128"]["fd_eps1e-4_within_1e-4"] = fd["eps_0.0001"]["cells_within_1e-4"]
+            out["adj128"]["fd_richardson_max_rel"] = _r(fd["richardson_h_0.005"]["max_rel_err"], 3)
+        if "fp32_vs_fp64_grad_l2_rel" in a:
+            out["adj128"]["fp32_vs_fp64"] = _r(a["fp32_vs_fp64_grad_l2_rel"], 3)
+    q = r.get("parity")
+    if q and "config0" in q:
+        out["parity"] = {c: {"rho": _r(q[c]["max_rel_err_rho"], 3), "u": _r(q[c]["max_rel_err_u"], 3),
+                             "bitwise": q[c]["bit_identical"], "steps": q[c]["steps"]}
+                         for c in ("config0", "config1")}
+    out["e2e_mlups"] = _r(r["e2e"]["value"])
+    cb = r.get("cpu_baseline")
+    if cb and cb.get("value"):
+        out["cpu_ref_mlups"] = _r(cb["value"])
+    return out
+
+
+# ---------------------------------------------------------------------------
+# parity at the stated sizes: configs 0 and 1 against LBM-Bench's own kernels
+# ---------------------------------------------------------------------------
+
+def parity_study(L, flags256, f0_256, steps256: int = 10):
+    """FP64 pull, push and AA on the GPU against the reference's own strict
+    pull-soa (oracle/_ref/libref_verify_l316: LBM-Bench's sources with
+    -DVERIFICATION, Lambda 3/16, -O2 -ffp-contract=off, OpenMP) run on this
+    host's cores, on the same inputs:
+      config0  64^3 channel, omega 1.25, F 1e-6, seeded +-1e-4
+               equilibrium, 1000 steps;
+      config1  the 256^3 porous benchmark workload, `steps256` steps.
+    Reports the normwise relative rho and u errors (the stated bound is
+    1e-12) and whether the states are bit-identical."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.ref_available("verify_l316"):
+        return {"unavailable": "oracle/_ref/libref_verify_l316.so not built"}
+    ref = O.Reference("verify_l316")
+    threads = ref.max_threads()
+    flags64, per64, _ = L.geometry("channel", (64, 64, 64))
+    f0_64 = L.perturbed_equilibrium(flags64, seed=7, amplitude=1e-4)
+    out = {}
+    for name, flags, per, f0, steps in (("config0", flags64, per64, f0_64, 1000),
+                                        ("config1", flags256, (1, 0, 0), f0_256, steps256)):
+        t0 = time.perf_counter()
+        r, _, _, _ = ref.run("pull-soa", flags, per, f0, steps, 1.25, 1e-6)
+        ref_s = time.perf_counter() - t0
+        m = O.fluid_mask(flags)
+        rows = {}
+        for pattern in ("aa", "pull", "push"):
+            sv = solver(L, flags, pattern, L.F64, f0)
+            sv.run(steps)
+            g = sv.get_state()
+            sv.close()
+            e_rho, e_u = O.normwise_errors(g, r, flags)
+            rows[pattern] = {"rel_err_rho": e_rho, "rel_err_u": e_u,
+                             "bit_identical": bool(np.array_equal(g[:, m], r[:, m]))}
+            del g
+        nz, ny, nx = flags.shape
+        out[name] = {
+            "dims": [nx, ny, nz], "steps": steps, "fluid_cells": int(m.sum()),
+            "max_rel_err_rho": max(v["rel_err_rho"] for v in rows.values()),
+            "max_rel_err_u": max(v["rel_err_u"] for v in rows.values()),
+            "bit_identical": all(v["bit_identical"] for v in rows.values()),
+            "bound": 1e-12, "patterns": rows,
+            "reference": f"LBM-Bench pull-soa, strict FP build (-DVERIFICATION, Lambda 3/16), "
+                         f"{threads} OpenMP threads, {ref_s:.1f} s"}
+        del r
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -518,17 +645,20 @@ def timed_forward(L, flags, pattern, precision, steps, warmup, peak):
                "bytes_per_update": s.bytes_per_update, "clocks": clk.summary()}
 
 
-def run_precision_study(args):
-    """512^3 porous channel, 300 steps: FP32 and FP16 storage of f - w
-    (FP32 arithmetic) against the FP64 run of the same seed."""
-    import lbmb200 as L
+def precision_study(L, n: int, steps: int, peak: float):
+    """n^3 porous channel (20% solid, r 4-8), `steps` steps: FP64 AA, and
+    FP32 and FP16 storage of f - w (FP32 arithmetic) in AA, each with the L2
+    relative u and rho errors against the FP64 run of the same seed."""
     import numpy as np
 
-    n, steps = args.size or 512, args.steps
     flags, frac, nsph = L.porous_channel((n, n, n), 0.2, 4.0, 8.0, seed=42)
-    peak, peak_kind = measured_hbm_peak()
     ref, r64 = timed_forward(L, flags, "aa", L.F64, steps, 0, peak)
-    res = {"fp64_aa": r64}
+    res = {"workload": f"precision study, porous channel {n}^3, 20% solid spheres r 4-8, "
+                       "seed 42", "dims": [n] * 3, "steps": steps,
+           "solid_fraction_achieved": frac, "spheres": nsph,
+           "init": "equilibrium +-1e-4 seed 7 (generated on the device)",
+           "error": f"L2 relative error of u and rho over fluid cells vs the FP64 AA run "
+                    f"after {steps} steps", "fp64_aa": r64}
     for name, prec in (("fp32", L.F32), ("fp16", L.F16)):
         b, r = timed_forward(L, flags, "aa", prec, steps, 0, peak)
         d = b.compare(ref)
@@ -537,18 +667,28 @@ def run_precision_study(args):
         r["speedup_vs_fp64_aa"] = r["mlups"] / r64["mlups"]
         res[f"{name}_aa"] = r
         b.close()
-    tot, bad = ref.mass_momentum(check=False)
+    _, bad = ref.mass_momentum(check=False)
+    res["fp64_nonfinite_cells"] = bad
     ref.close()
-    wl = {"workload": f"precision study, porous channel {n}^3, 20% solid spheres r 4-8, seed 42",
-          "dims": [n] * 3, "solid_fraction_achieved": frac, "spheres": nsph,
+    return res
+
+
+def run_precision_study(args):
+    """512^3 porous channel, 300 steps: FP32 and FP16 storage of f - w
+    (FP32 arithmetic) against the FP64 run of the same seed."""
+    import lbmb200 as L
+
+    n, steps = args.size or 512, args.steps
+    peak, peak_kind = measured_hbm_peak()
+    res = precision_study(L, n, steps, peak)
+    wl = {"workload": res["workload"], "dims": [n] * 3,
+          "solid_fraction_achieved": res["solid_fraction_achieved"], "spheres": res["spheres"],
           "steps": steps, "omega": 1.25, "lambda": 3 / 16, "xforce": 1e-6,
-          "init": "equilibrium +-1e-4 seed 7 (generated on the device)",
-          "error": "L2 relative error of u and rho over fluid cells vs the FP64 run after "
-                   f"{steps} steps", "hbm_peak_gbs": peak, "hbm_peak_source": peak_kind,
-          "l2_flush": "not needed: states of 5-20 GB > 126 MB L2"}
+          "init": res["init"], "error": res["error"], "hbm_peak_gbs": peak,
+          "hbm_peak_source": peak_kind, "l2_flush": "not needed: states of 5-20 GB > 126 MB L2"}
     f16 = res["fp16_aa"]
     return base_line(f16["mlups"], "MLUPS", steps, 0, f16["ms_per_step"], wl, "f32 (f16 storage)",
-                     {"variants": res, "fp64_nonfinite_cells": bad})
+                     {"variants": res})
 
 
 def run_adjoint_only(args):
@@ -559,6 +699,25 @@ def run_adjoint_only(args):
                      {"adjoint": a})
 
 
+def largest_study(L, n: int, steps: int, peak: float, na: int = 384, adj_steps: int = 1000):
+    """The n^3 FP16 forward (30% solid, r 6-12, AA) and the na^3 FP32
+    Brinkman adjoint with the sqrt checkpoint schedule, with device memory
+    against the 180 GB HBM."""
+    flags, frac, nsph = L.porous_channel((n, n, n), 0.3, 6.0, 12.0, seed=42)
+    free0, total = L.device_memory()
+    s, fwd = timed_forward(L, flags, "aa", L.F16, steps, 3, peak)
+    free1, _ = L.device_memory()
+    _, bad = s.mass_momentum(check=False)
+    fwd.update({"workload": f"FP16 porous channel {n}^3 (30% solid, r 6-12), AA, {steps} steps",
+                "nonfinite_cells": bad, "device_used_bytes": total - free1,
+                "device_total_bytes": total, "solid_fraction_achieved": frac, "spheres": nsph})
+    s.close()
+    del flags
+    a = adjoint_study(L, na, adj_steps, 0, 0, precisions=("fp32",))
+    a["fp32"]["device_total_bytes"] = total
+    return {"forward_fp16_aa": fwd, "adjoint": a}
+
+
 def run_largest(args):
     """768^3 FP16 forward (30% solid, r 6-12, 200 steps) and the 384^3
     FP32 Brinkman adjoint with the sqrt checkpoint schedule (1000 steps)."""
@@ -566,24 +725,14 @@ def run_largest(args):
 
     n = args.size or 768
     peak, peak_kind = measured_hbm_peak()
-    flags, frac, nsph = L.porous_channel((n, n, n), 0.3, 6.0, 12.0, seed=42)
-    free0, total = L.device_memory()
-    s, fwd = timed_forward(L, flags, "aa", L.F16, args.steps, 3, peak)
-    free1, _ = L.device_memory()
-    tot, bad = s.mass_momentum(check=False)
-    fwd.update({"nonfinite_cells": bad, "device_used_bytes": total - free1,
-                "device_total_bytes": total, "solid_fraction_achieved": frac, "spheres": nsph})
-    s.close()
-    del flags
-    na = 384
-    a = adjoint_study(L, na, 1000, 0, 0, precisions=("fp32",))
-    a["fp32"]["device_total_bytes"] = total
+    res = largest_study(L, n, args.steps, peak)
+    fwd = res["forward_fp16_aa"]
     wl = {"workload": f"largest single-GPU sizes: FP16 porous channel {n}^3 (30% solid, r 6-12), "
-                      f"{args.steps} steps; FP32 Brinkman adjoint {na}^3, 1000 steps, sqrt "
+                      f"{args.steps} steps; FP32 Brinkman adjoint 384^3, 1000 steps, sqrt "
                       "checkpoint schedule",
           "hbm_peak_gbs": peak, "hbm_peak_source": peak_kind, "hbm_capacity_gb": 180}
     return base_line(fwd["mlups"], "MLUPS", args.steps, 3, fwd["ms_per_step"], wl,
-                     "f32 (f16 storage)", {"forward_fp16_aa": fwd, "adjoint": a})
+                     "f32 (f16 storage)", res)
 
 
 def run_slabs(args, dist: Dist):
@@ -737,6 +886,30 @@ def run_reference(args):
     }
 
 
+def run_profile_case(args):
+    """A short run of the step kernels for profilers (ncu): the n^3 porous
+    channel of the benchmark, for each precision in turn the seeded initial
+    state uploaded (mask_kernel, then 19 pack_plane_kernel launches) and
+    `--steps` steps of the pattern (AA alternates even, odd, ...). Prints
+    one progress line per precision to standard error, no JSON line."""
+    import lbmb200 as L
+
+    pattern, _, precs = args.profile_run.partition(":")
+    n = args.size
+    flags, _, _ = L.porous_channel((n, n, n), 0.2, 4.0, 8.0, seed=42)
+    f0 = L.perturbed_equilibrium(flags, seed=7, amplitude=1e-4)
+    for prec in (precs or "fp64").split(","):
+        with L.Solver(flags, (1, 0, 0), pattern, L.PRECISIONS[prec]) as s:
+            s.set_params(1.25, 3 / 16, 1e-6, True)
+            s.set_state(f0)
+            ms = s.run_timed(args.steps)
+            _, bad = s.mass_momentum(check=False)
+            log(f"{n}^3 {pattern} {prec}: {s.fluid_cells} fluid cells, {args.steps} steps in "
+                f"{ms:.3f} ms, {s.bytes_per_update:.0f} B/update, nonfinite {bad}")
+            if bad:
+                raise SystemExit("non-finite populations")
+
+
 def _json_channel():
     """The one JSON line goes to the process's standard output; everything
     else written to file descriptor 1 - the C libraries' progress lines, the
@@ -758,10 +931,20 @@ def main():
                     help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-studies", action="store_true",
+                    help="skip the 512^3 precision study and the largest sizes")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the comparison with the reference at configs 0 and 1")
+    ap.add_argument("--profile-run", metavar="PATTERN:PRECISIONS",
+                    help="profiling case, e.g. aa:fp64,fp16 - `--steps` steps of the "
+                         "pattern on the --size^3 porous channel, no JSON line")
     ap.add_argument("--config", type=int, choices=[1, 2, 3, 4], default=1,
                     help="1: 256^3 patterns (default); 2: 512^3 precision study; "
                          "3: 128^3 adjoint; 4: 768^3 FP16 and 384^3 adjoint")
     args = ap.parse_args()
+    if args.profile_run:
+        run_profile_case(args)
+        return
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     out = _json_channel()

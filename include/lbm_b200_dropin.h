@@ -138,6 +138,19 @@ void lbmB200SetMagicParameter(double lambda);
  * reference's benchmark build). */
 void lbmB200SetBodyForce(int on);
 
+/* The reference's -DVERIFICATION build applies the body force inside its
+ * own kernels (src/kernel_pull_soa.c:206-209). A translation unit of such a
+ * build that includes this header (LBM-Bench's lbm.c, once the rows are
+ * added to GKernels[]) switches the drop-in's body force on when the program
+ * loads, so -V works with no further change; a later lbmB200SetBodyForce
+ * call still overrides it. */
+#if defined(VERIFICATION) && defined(__GNUC__)
+__attribute__((constructor)) static void lbmB200VerificationBuild(void)
+{
+  lbmB200SetBodyForce(1);
+}
+#endif
+
 #ifdef __cplusplus
 }
 #endif

@@ -397,3 +397,23 @@ def counter_equilibrium(flags, seed, amplitude=1e-4, rho=1.0):
         f[d] = W[d] * (((rho - 1.5 * usq) + 3.0 * cu) + 4.5 * cu * cu)
         f[d][~fluid] = 0.0
     return f
+
+
+def normwise_errors(f, ref, flags):
+    """Normwise relative errors of density and velocity of state f against
+    state ref over the fluid cells: ||rho - rho_ref||_2 / ||rho_ref||_2 and
+    ||u - u_ref||_2 / ||u_ref||_2 with u = j / rho the velocity vector
+    (j the momentum sum_d c_d f_d). Returns (err_rho, err_u)."""
+    m = fluid_mask(flags)
+
+    def rho_u(a):
+        rho = a[:, m].sum(axis=0)
+        j = [np.tensordot(c.astype(np.float64), a[:, m], axes=(0, 0)) for c in (CX, CY, CZ)]
+        return rho, [v / rho for v in j]
+
+    r1, u1 = rho_u(f)
+    r0, u0 = rho_u(ref)
+    e_rho = float(np.linalg.norm(r1 - r0) / np.linalg.norm(r0))
+    du = np.sqrt(sum(float(((a - b) ** 2).sum()) for a, b in zip(u1, u0)))
+    nu = np.sqrt(sum(float((b * b).sum()) for b in u0))
+    return e_rho, float(du / nu)

@@ -11,11 +11,14 @@ For every case the script
     and blocked variants for the first cases) and checks they agree bit for
     bit,
   * records the SHA-256 of the final state over fluid cells and some totals.
-It also records the reference's Poiseuille verification (-V) result, and
-two pressure-driven channels run with the reference's Zou-He boundary pass
-after every pull and push step.
+It also records the reference's Poiseuille verification (-V) result, two
+pressure-driven channels run with the reference's Zou-He boundary pass
+after every pull and push step, and the stated config-0 case at full size:
+a 64^3 channel, omega 1.25, Lambda 3/16, F 1e-6, the counter-based seeded
++-1e-4 equilibrium of the benchmark, 1000 steps (several minutes of CPU).
 
-Usage: python tests/golden/make_golden.py
+Usage: python tests/golden/make_golden.py [--only NAME ...]
+  --only regenerates the named cases and keeps every other stored case.
 """
 import json
 import os
@@ -68,8 +71,13 @@ def porous_flags(dims, fraction, rmin, rmax, seed):
     return flags
 
 
+# The 64^3 channel of the first benchmark configuration, at its stated size.
+CONFIG0 = ("config0_channel64", "channel", (64, 64, 64), (0, 0, 0), 1.25, 3 / 16, 1e-6, 1, 1000,
+           7, "verify_l316")
+
+
 def run_case(name, geo, dims, pin, omega, lam, xforce, force, steps, seed, variant, arrays,
-             flags=None):
+             flags=None, init="rng"):
     ref = O.Reference(variant)
     if flags is None:
         flags, per, counts = ref.geometry(geo, dims, pin)
@@ -77,7 +85,8 @@ def run_case(name, geo, dims, pin, omega, lam, xforce, force, steps, seed, varia
         assert np.array_equal(mine, flags), f"{name}: numpy geometry restatement differs"
     else:
         per = (1, 0, 0)
-    f0 = O.perturbed_state(flags, seed)
+    f0 = O.counter_equilibrium(flags, seed) if init == "counter" else \
+        O.perturbed_state(flags, seed)
     kernels = ["pull-soa", "push-soa", "aa-soa"]
     if name in ALL_KERNELS:
         kernels = ref.kernels()
@@ -101,6 +110,11 @@ def run_case(name, geo, dims, pin, omega, lam, xforce, force, steps, seed, varia
         "mass": float(rho[m].sum()), "momentum": [float(ux[m].sum()), float(uy[m].sum()),
                                                   float(uz[m].sum())],
     }
+    if init == "counter":
+        case["init"] = "counter"
+        vel = [a[m] / rho[m] for a in (ux, uy, uz)]
+        case["norms"] = {"rho_l2": float(np.linalg.norm(rho[m])),
+                         "u_l2": float(np.sqrt(sum(float((v * v).sum()) for v in vel)))}
     if name in FULL_STATE:
         arrays[f"{name}_f"] = base
         case["state_key"] = f"{name}_f"
@@ -159,7 +173,24 @@ def run_pressure_case(name, dims, solid, seed, omega, lam, xforce, force, steps,
 
 
 def main():
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", nargs="*", default=None)
+    only = ap.parse_args().only
     O.build()
+    if only:
+        cases, stored = golden_io.load()
+        arrays = {k: stored[k] for k in stored.files}
+        for name in only:
+            if name != CONFIG0[0]:
+                raise SystemExit(f"--only supports {CONFIG0[0]}")
+            case, _ = run_case(*CONFIG0, arrays=arrays, init="counter")
+            cases = [c for c in cases if c["name"] != name] + [case]
+            print(case["name"], case["sha256"][:16], case["n_fluid"])
+        with open(golden_io.CASES_JSON, "w") as fh:
+            json.dump(cases, fh, indent=1)
+        np.savez_compressed(golden_io.ARRAYS_NPZ, **arrays)
+        return
     arrays = {}
     cases = []
     for row in CASES:
@@ -199,6 +230,10 @@ def main():
                   "initial_key": "verify_initial_f", "reference_build": "verify",
                   "verify": verify, "sha256": verify["pull-soa"]["sha256"]})
     print("poiseuille", verify)
+
+    case, _ = run_case(*CONFIG0, arrays=arrays, init="counter")
+    cases.append(case)
+    print(case["name"], case["sha256"][:16], case["n_fluid"])
 
     with open(golden_io.CASES_JSON, "w") as fh:
         json.dump(cases, fh, indent=1)

@@ -89,6 +89,11 @@ def effective_periodic(case: dict):
 
 
 def initial_state(case: dict, flags: np.ndarray) -> np.ndarray:
+    """The case's seeded perturbed equilibrium: the counter-based generator
+    of the benchmark (init "counter", the product's lbm_perturbed_equilibrium
+    restated) or numpy's default generator (every other case)."""
+    if case.get("init") == "counter":
+        return O.counter_equilibrium(flags, case["seed"], case.get("amp", 1e-4))
     return O.perturbed_state(flags, case["seed"], amp=case.get("amp", 1e-4))
 
 

@@ -14,7 +14,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "lbm-bench_b200")
 CLI = os.path.join(PKG, "lbmbench-b200")
 PROBE = os.path.join(ROOT, "tests", "dropin_layout_probe.c")
-REF_SRC = "/root/reference/src"
+# the reference's own src/lbm.h: the unmodified build-time copy that
+# oracle/Makefile takes of the reference sources next to its drop-in build
+REF_SRC = os.path.join(ROOT, "oracle", "_ref", "dropin_src-dp")
 
 
 def _probe(tmp_path, *flags):
@@ -32,7 +34,7 @@ def test_dropin_types_compile_and_link_standalone(tmp_path):
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(REF_SRC, "lbm.h")),
-                    reason="reference sources not mounted here")
+                    reason="oracle/_ref not built (needs the reference sources)")
 @pytest.mark.parametrize("sp", [False, True])
 def test_dropin_struct_layout_equals_reference_lbm_h(tmp_path, sp):
     extra = ["-DPRECISION_SP"] if sp else []
@@ -99,3 +101,22 @@ def test_cli_fails_loudly_without_gpu():
     r = subprocess.run([CLI, "-d", "8x8x8"], capture_output=True, text=True)
     assert r.returncode != 0
     assert "no CPU path" in r.stdout
+
+
+REF_DROPIN = {p: os.path.join(ROOT, "oracle", "_ref", f"lbmbench-dropin-{p}") for p in ("dp", "sp")}
+
+
+@pytest.mark.parametrize("prec", ["dp", "sp"])
+def test_reference_binary_with_dropin_rows_lists_all_kernels(prec):
+    """LBM-Bench's own binary (its main.c/cli.c, oracle/Makefile) with the
+    drop-in rows appended to GKernels[]: `-l` lists the reference's seven
+    names in its order, then the 13 cuda-* rows, parsed the way
+    src/test.sh:95 parses it. No GPU is touched by -l."""
+    exe = REF_DROPIN[prec]
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref/lbmbench-dropin-* not built (needs the reference sources)")
+    out = subprocess.run([exe, "-l"], capture_output=True, text=True, check=True).stdout
+    lines = out.splitlines()
+    start = lines.index("Available kernels:")
+    names = [ln.split()[0] for ln in lines[start + 1:] if ln.strip()]
+    assert names == REFERENCE_NAMES + L.dropin_kernels()

@@ -161,3 +161,40 @@ def test_cli_verification_run_succeeds(kernel):
         assert err == pytest.approx(ref["error_norm"], rel=1e-6)
     else:
         assert err < 0.06
+
+
+REF_DROPIN = {p: os.path.join(ROOT, "oracle", "_ref", f"lbmbench-dropin-{p}") for p in ("dp", "sp")}
+
+
+def _kernels_listed(exe):
+    out = subprocess.run([exe, "-l"], capture_output=True, text=True, check=True).stdout
+    lines = out.splitlines()
+    return [ln.split()[0] for ln in lines[lines.index("Available kernels:") + 1:] if ln.strip()]
+
+
+@pytest.mark.parametrize("prec", ["dp", "sp"])
+def test_reference_binary_with_dropin_rows_passes_its_own_verification(prec):
+    """The reference's own driver, linked against liblbmb200 with the
+    drop-in rows in GKernels[] and nothing else changed (oracle/Makefile):
+    what src/test.sh:95-103 does - `-V -k K` for every kernel `-l` lists,
+    exit status 0 - for the reference's seven names and the 13 cuda-* rows.
+    In the double build the cuda pull/push/AA names (all FP64) give exactly
+    the error norm the same binary's own kernels give."""
+    exe = REF_DROPIN[prec]
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref/lbmbench-dropin-* not built (needs the reference sources)")
+    errs = {}
+    for k in _kernels_listed(exe):
+        r = subprocess.run([exe, "-V", "-k", k], capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, (k, r.stdout[-2000:] + r.stderr[-2000:])
+        assert "# VERIFICATION SUCCEEDED." in r.stdout, k
+        errs[k] = float(re.search(r"deviation from analytical solution: (\S+)",
+                                  r.stdout).group(1))
+    assert len(errs) == 20
+    if prec == "dp":
+        for k in ("cuda-pull-soa", "cuda-push-soa", "cuda-aa-soa", "cuda-pull-aos",
+                  "cuda-push-aos", "cuda-blk-push-soa", "cuda-blk-pull-soa"):
+            assert errs[k] == errs["aa-soa"], (k, errs[k], errs["aa-soa"])
+        assert errs["aa-soa"] == pytest.approx(4.5614e-2, rel=1e-4)
+    for k in errs:
+        assert errs[k] < 0.06, (k, errs[k])
