@@ -263,8 +263,8 @@ def workload_config(n, frac, nsph, n_fluid):
     return cfg
 
 
-def solver(L, flags, pattern, precision, f0):
-    s = L.Solver(flags, (1, 0, 0), pattern, precision)
+def solver(L, flags, pattern, precision, f0, compact=False):
+    s = L.Solver(flags, (1, 0, 0), pattern, precision, compact=compact)
     s.set_params(1.25, 3 / 16, 1e-6, True)
     s.set_state(f0)
     return s
@@ -283,7 +283,9 @@ def run_native(args, dist: Dist):
     peak, peak_kind = measured_hbm_peak()
 
     # ---- headline: FP64 AA, device-resident, timed region with per-launch events
-    s = solver(L, flags, "aa", L.F64, f0)
+    compact = args.layout == "compact"
+    other = "dense" if compact else "compact"
+    s = solver(L, flags, "aa", L.F64, f0, compact)
     n_fluid = s.fluid_cells
     bpu = s.bytes_per_update
     s.run(args.warmup)
@@ -302,8 +304,10 @@ def run_native(args, dist: Dist):
     dom = max(per_kind, key=lambda k: per_kind[k][0])
     dom_ms = per_kind[dom][0] / per_kind[dom][1]
     achieved = n_fluid * bpu / (dom_ms / 1e3) / 1e9
-    traffic = ncu_traffic(dom, "fp64")
-    roofline = {"bound": "hbm", "kernel": f"step_kernel<StoreF64,{dom}>", "achieved": achieved,
+    traffic = ncu_traffic(dom, "fp64_compact" if compact else "fp64")
+    kname = (("step_kernel_cp_local<StoreF64>" if dom == "aa_even" else
+              f"step_kernel_cp<StoreF64,{dom}>") if compact else f"step_kernel<StoreF64,{dom}>")
+    roofline = {"bound": "hbm", "kernel": kname, "layout": args.layout, "achieved": achieved,
                 "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic * n_fluid if traffic else None,
                 "algorithmic_bytes_per_launch": n_fluid * bpu,
@@ -313,16 +317,21 @@ def run_native(args, dist: Dist):
     variants = {}
     vsteps = max(20, args.steps // 2)
     ref64 = s  # FP64 AA solver; compare after equal step counts
-    for pattern in ("pull", "push"):
-        v = solver(L, flags, pattern, L.F64, f0)
+    # FP64 in both layouts (the headline's layout without a suffix)
+    for pattern, cp in (("pull", compact), ("push", compact), ("aa", not compact),
+                        ("pull", not compact), ("push", not compact)):
+        v = solver(L, flags, pattern, L.F64, f0, cp)
         v.run(args.warmup)
         t = v.run_timed(vsteps)
-        variants[f"fp64_{pattern}"] = {
+        key = f"fp64_{pattern}" + ("" if cp == compact else f"_{other}")
+        variants[key] = {
             "mlups": n_fluid * vsteps / (t / 1e3) / 1e6,
-            "gbs": n_fluid * vsteps * v.bytes_per_update / (t / 1e3) / 1e9}
-        variants[f"fp64_{pattern}"]["frac"] = variants[f"fp64_{pattern}"]["gbs"] / peak
+            "gbs": n_fluid * vsteps * v.bytes_per_update / (t / 1e3) / 1e9,
+            "layout": "compact" if cp else "dense", "device_bytes": v.device_bytes}
+        variants[key]["frac"] = variants[key]["gbs"] / peak
         v.close()
-    ref = solver(L, flags, "aa", L.F64, f0)  # accuracy reference: FP64, same seed
+    # FP32 / FP16 storage in the dense layout (its multi-cell kernels are faster there)
+    ref = solver(L, flags, "aa", L.F64, f0, compact)  # accuracy reference: FP64, same seed
     ref.run(args.steps)
     for name, prec in (("fp32", L.F32), ("fp16", L.F16)):
         for pattern in ("aa", "pull"):
@@ -336,7 +345,7 @@ def run_native(args, dist: Dist):
                 "mlups": mlups, "gbs": mlups * b.bytes_per_update / 1e3 if mlups else None,
                 "l2_rel_err_u": float(np.sqrt(d[0] / d[1])) if d[1] > 0 else None,
                 "l2_rel_err_rho": float(np.sqrt(d[2] / d[3])) if d[3] > 0 else None,
-                "error_after_steps": args.steps}
+                "error_after_steps": args.steps, "layout": "dense"}
             if mlups:
                 variants[key]["frac"] = variants[key]["gbs"] / peak
                 variants[key]["speedup_vs_fp64_aa"] = mlups / (value / dist.world)
@@ -395,8 +404,10 @@ def summary(r):
     adjoint's cost, and the parity of configs 0 and 1 with the reference."""
     v = r.get("variants", {})
     out = {"fp64_aa": {"mlups": _r(r["value"]), "frac_step": _r(r["gbs"] / r["roofline"]["peak"]),
-                       "frac_odd": _r(r["roofline"]["frac"])}}
-    for k in ("fp64_pull", "fp64_push"):
+                       "frac_dominant": _r(r["roofline"]["frac"]),
+                       "layout": r["roofline"].get("layout")}}
+    for k in ("fp64_pull", "fp64_push", "fp64_aa_dense", "fp64_pull_dense", "fp64_push_dense",
+              "fp64_aa_compact", "fp64_pull_compact", "fp64_push_compact"):
         if k in v:
             out[k] = {"mlups": _r(v[k]["mlups"]), "frac": _r(v[k]["frac"])}
     for k in ("fp32_aa", "fp32_pull", "fp16_aa", "fp16_pull"):
@@ -406,7 +417,8 @@ def summary(r):
                       "err_u": _r(v[k]["l2_rel_err_u"], 2), "err_rho": _r(v[k]["l2_rel_err_rho"], 2)}
     p = r.get("precision_512")
     if p:
-        out["p512"] = {"fp64_aa": _r(p["fp64_aa"]["mlups"])}
+        out["p512"] = {"fp64_aa": _r(p["fp64_aa"]["mlups"]),
+                       "fp64_aa_dense": _r(p["fp64_aa_dense"]["mlups"])}
         for k in ("fp32_aa", "fp16_aa"):
             out["p512"][k] = {"mlups": _r(p[k]["mlups"]), "frac": _r(p[k]["frac"]),
                               "x_fp64_aa": _r(p[k]["speedup_vs_fp64_aa"], 3),
@@ -630,8 +642,8 @@ def base_line(metric_value, unit, steps, warmup, ms, workload, dtype, extra):
     return r
 
 
-def timed_forward(L, flags, pattern, precision, steps, warmup, peak):
-    s = L.Solver(flags, (1, 0, 0), pattern, precision)
+def timed_forward(L, flags, pattern, precision, steps, warmup, peak, compact=False):
+    s = L.Solver(flags, (1, 0, 0), pattern, precision, compact=compact)
     s.set_params(1.25, 3 / 16, 1e-6, True)
     s.init_equilibrium(seed=7, amplitude=1e-4)
     s.run(warmup)
@@ -642,7 +654,8 @@ def timed_forward(L, flags, pattern, precision, steps, warmup, peak):
     gbs = mlups * s.bytes_per_update / 1e3
     return s, {"mlups": mlups, "gbs": gbs, "frac": gbs / peak, "ms_per_step": ms / steps,
                "fluid_cells": n_fluid, "device_bytes": s.device_bytes,
-               "bytes_per_update": s.bytes_per_update, "clocks": clk.summary()}
+               "bytes_per_update": s.bytes_per_update, "clocks": clk.summary(),
+               "layout": "compact" if compact else "dense"}
 
 
 def precision_study(L, n: int, steps: int, peak: float):
@@ -652,13 +665,15 @@ def precision_study(L, n: int, steps: int, peak: float):
     import numpy as np
 
     flags, frac, nsph = L.porous_channel((n, n, n), 0.2, 4.0, 8.0, seed=42)
-    ref, r64 = timed_forward(L, flags, "aa", L.F64, steps, 0, peak)
+    d64, r64d = timed_forward(L, flags, "aa", L.F64, steps, 0, peak)
+    d64.close()
+    ref, r64 = timed_forward(L, flags, "aa", L.F64, steps, 0, peak, compact=True)
     res = {"workload": f"precision study, porous channel {n}^3, 20% solid spheres r 4-8, "
                        "seed 42", "dims": [n] * 3, "steps": steps,
            "solid_fraction_achieved": frac, "spheres": nsph,
            "init": "equilibrium +-1e-4 seed 7 (generated on the device)",
            "error": f"L2 relative error of u and rho over fluid cells vs the FP64 AA run "
-                    f"after {steps} steps", "fp64_aa": r64}
+                    f"after {steps} steps", "fp64_aa": r64, "fp64_aa_dense": r64d}
     for name, prec in (("fp32", L.F32), ("fp16", L.F16)):
         b, r = timed_forward(L, flags, "aa", prec, steps, 0, peak)
         d = b.compare(ref)
@@ -899,7 +914,8 @@ def run_profile_case(args):
     flags, _, _ = L.porous_channel((n, n, n), 0.2, 4.0, 8.0, seed=42)
     f0 = L.perturbed_equilibrium(flags, seed=7, amplitude=1e-4)
     for prec in (precs or "fp64").split(","):
-        with L.Solver(flags, (1, 0, 0), pattern, L.PRECISIONS[prec]) as s:
+        with L.Solver(flags, (1, 0, 0), pattern, L.PRECISIONS[prec],
+                      compact=args.layout == "compact") as s:
             s.set_params(1.25, 3 / 16, 1e-6, True)
             s.set_state(f0)
             ms = s.run_timed(args.steps)
@@ -938,6 +954,9 @@ def main():
     ap.add_argument("--profile-run", metavar="PATTERN:PRECISIONS",
                     help="profiling case, e.g. aa:fp64,fp16 - `--steps` steps of the "
                          "pattern on the --size^3 porous channel, no JSON line")
+    ap.add_argument("--layout", choices=["dense", "compact"], default="compact",
+                    help="storage layout of the FP64 headline and of --profile-run "
+                         "(compact: fluid cells only; default)")
     ap.add_argument("--config", type=int, choices=[1, 2, 3, 4], default=1,
                     help="1: 256^3 patterns (default); 2: 512^3 precision study; "
                          "3: 128^3 adjoint; 4: 768^3 FP16 and 384^3 adjoint")

@@ -72,6 +72,20 @@ int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *flags, int p
 int lbm_create_slab(lbm_solver **out, int nx, int ny, int nz, const int *flags, int periodic_y,
     int periodic_z, int pattern, int precision);
 
+/* The same solver in the compact (fluid-only) layout: populations and link
+ * masks are stored for fluid cells only, packed row by row in z order, so no
+ * obstacle cell shares a memory sector with a fluid one and every byte moved
+ * belongs to a fluid cell. The reference sweeps its dense box
+ * (src/kernel_pull_soa.c:94-96) and has no such layout. Results are
+ * identical to lbm_create's (FP64: bit for bit, like the reference); every
+ * call below works on it except lbm_set_porosity / lbm_adjoint_gradient
+ * (no Brinkman term) and the slab calls. */
+int lbm_create_compact(lbm_solver **out, int nx, int ny, int nz, const int *flags,
+    int periodic_x, int periodic_y, int periodic_z, int pattern, int precision);
+
+/* 1 if the solver uses the compact layout, 0 if not, -1 for NULL. */
+int lbm_is_compact(const lbm_solver *s);
+
 /* Frees everything the solver owns (src/lbm.c:660-670). NULL is a no-op. */
 int lbm_destroy(lbm_solver *s);
 

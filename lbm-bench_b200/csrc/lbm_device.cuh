@@ -173,11 +173,23 @@ __device__ __forceinline__ void collide(const V (&f)[Q], V (&o)[Q], const Consts
 // neighbour always exists and a bounced population always has a wall slot
 // to sit in (as in the reference's obstacle and ghost slots,
 // src/lbm.c:532-566).
+//
+// Compact ("fluid-only") layout, when `bits` is set: only fluid cells hold
+// storage. The fluid cells of one (x, y) row sit consecutively in z order,
+// rows follow in (x, y) order, and a cell's storage index is its rank among
+// all fluid cells. Per row, W 32-bit words hold one fluid bit per z (bit
+// z % 32 of word z / 32), and base[] holds for every word the index of the
+// first fluid cell at or after z = 32 w, so a fluid cell's index is
+// base + popc(word & bits below z). Plane stride and mask array then count
+// fluid cells only; no solid cell shares a 32-byte sector with a fluid one.
 struct Grid {
   int nx, ny, nz;  // device extent (the caller's box plus frames)
   int pz;          // z pitch of a row, elements
   int per;         // periodic axes: bit 0 x, bit 1 y, bit 2 z
   long long plane; // elements per direction plane
+  const uint32_t *bits = nullptr; // compact layout: fluid bits [nx*ny rows][W]
+  const uint32_t *base = nullptr; // compact layout: first index at or after each word
+  int W = 0;                      // compact layout: words per row
 };
 
 // Caller's box inside the device box: offsets and extent.
@@ -232,9 +244,87 @@ __device__ __forceinline__ Offs make_offs(const Grid &g, int x, int y, int z)
   return o;
 }
 
+// Compact layout: storage index of the fluid cell (x, y, z) (device
+// coordinates; the cell must be fluid).
+__device__ __forceinline__ uint32_t packed_index(const Grid &g, int x, int y, int z)
+{
+  const uint32_t k =
+      ((uint32_t)x * (uint32_t)g.ny + (uint32_t)y) * (uint32_t)g.W + (uint32_t)(z >> 5);
+  return __ldg(g.base + k) + (uint32_t)__popc(__ldg(g.bits + k) & ((1u << (z & 31)) - 1u));
+}
+
+// Storage index and link mask of the device cell (x, y, z) in either
+// layout; false for a cell that is not updated (obstacle, frame, padding,
+// ghost plane).
+__device__ __forceinline__ bool locate(const Grid &g, const uint32_t *mask, int x, int y, int z,
+    uint32_t &cell, uint32_t &m)
+{
+  if (g.bits) {
+    const uint32_t k =
+        ((uint32_t)x * (uint32_t)g.ny + (uint32_t)y) * (uint32_t)g.W + (uint32_t)(z >> 5);
+    const uint32_t w = __ldg(g.bits + k);
+    if (!((w >> (z & 31)) & 1u))
+      return false;
+    cell = __ldg(g.base + k) + (uint32_t)__popc(w & ((1u << (z & 31)) - 1u));
+  } else {
+    cell = cell_index(g, x, y, z);
+  }
+  m = mask[cell];
+  return !(m & kSolidBit);
+}
+
+// Neighbours of one fluid cell in either layout: at(d) is the storage
+// index of x + c_d (wrapped across periodic axes), meaningful only when
+// that neighbour is fluid (mask bit d clear).
+struct Nbr {
+  Offs o;
+  uint32_t cell;
+  int x, y, z;
+  const Grid *g;
+  __device__ __forceinline__ uint32_t at(int d) const
+  {
+    if (!g->bits)
+      return cell + o.at(d);
+    int a = x + cx(d), b = y + cy(d), c = z + cz(d);
+    a = a < 0 ? g->nx - 1 : a >= g->nx ? 0 : a;
+    b = b < 0 ? g->ny - 1 : b >= g->ny ? 0 : b;
+    c = c < 0 ? g->nz - 1 : c >= g->nz ? 0 : c;
+    return packed_index(*g, a, b, c);
+  }
+};
+
+__device__ __forceinline__ Nbr make_nbr(const Grid &g, int x, int y, int z, uint32_t cell)
+{
+  Nbr n;
+  n.o = make_offs(g, x, y, z);
+  n.cell = cell;
+  n.x = x;
+  n.y = y;
+  n.z = z;
+  n.g = &g;
+  return n;
+}
+
 // Where f_d(x) of a fluid cell lives in a state of orientation `o` (plane
 // index, cell index). A population that bounced off the wall x - c_d is kept
 // in a slot of the cell itself that no neighbour uses.
+__device__ __forceinline__ void state_slot(int o, int d, uint32_t mask, uint32_t cell,
+    const Nbr &n, int &plane_out, uint32_t &cell_out)
+{
+  const bool back = (mask >> inv(d)) & 1u; // x - c_d is a wall
+  if (o == kNatural) {
+    plane_out = d;
+    cell_out = cell;
+  } else if (o == kPullState) {
+    plane_out = back ? inv(d) : d;
+    cell_out = back ? cell : n.at(inv(d));
+  } else {
+    plane_out = back ? d : inv(d);
+    cell_out = back ? cell : n.at(inv(d));
+  }
+}
+
+// The same with the dense layout's neighbour offsets.
 __device__ __forceinline__ void state_slot(int o, int d, uint32_t mask, uint32_t cell,
     const Offs &n, int &plane_out, uint32_t &cell_out)
 {

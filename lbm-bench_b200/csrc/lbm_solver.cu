@@ -87,6 +87,10 @@ struct lbm_solver {
   int split;             // a split step is open
   uint8_t *split_done;   // host: x planes of the open step already launched (nx bytes)
   int split_left;        // planes still to launch
+  // compact (fluid-only) layout: fluid bits and word bases per row (Grid)
+  int compact;
+  uint32_t *cbits, *cbase;
+  std::vector<uint32_t> *cplane0; // storage index of the first fluid cell of each x plane (nx+1)
 };
 
 extern "C" const char *lbm_last_error(void) { return g_err; }
@@ -231,6 +235,21 @@ __global__ void mask_kernel(Grid g, const uint8_t *fluid, uint32_t *mask, int gh
   mask[cell] = m;
 }
 
+// Compact layout: the dense link masks of the fluid cells, moved to their
+// storage indices.
+__global__ void compact_mask_kernel(Grid g, const uint32_t *__restrict__ dense_mask,
+    uint32_t *mask)
+{
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= g.nz || y >= g.ny)
+    return;
+  const uint32_t m = dense_mask[cell_index(g, x, y, z)];
+  if (!(m & kSolidBit))
+    mask[packed_index(g, x, y, z)] = m;
+}
+
 // Index of caller cell (x, y, z) in the caller's dense arrays.
 __device__ __forceinline__ long long dense_index(const UserBox &u, int x, int y, int z)
 {
@@ -249,11 +268,10 @@ __global__ void pack_plane_kernel(Grid g, UserBox u, int d, int orient,
   const int x = blockIdx.z;
   if (z >= u.nz || y >= u.ny)
     return;
-  const uint32_t cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
-  const uint32_t m = mask[cell];
-  if (m & kSolidBit)
+  uint32_t cell, m;
+  if (!locate(g, mask, x + u.ox, y + u.oy, z + u.oz, cell, m))
     return;
-  const Offs nb = make_offs(g, x + u.ox, y + u.oy, z + u.oz);
+  const Nbr nb = make_nbr(g, x + u.ox, y + u.oy, z + u.oz, cell);
   int p;
   uint32_t c;
   state_slot(orient, d, m, cell, nb, p, c);
@@ -275,13 +293,12 @@ __global__ void unpack_plane_kernel(Grid g, UserBox u, int d, int orient,
   const int x = blockIdx.z;
   if (z >= u.nz || y >= u.ny)
     return;
-  const uint32_t cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
-  const uint32_t m = mask[cell];
-  if (m & kSolidBit) {
+  uint32_t cell, m;
+  if (!locate(g, mask, x + u.ox, y + u.oy, z + u.oz, cell, m)) {
     dense[dense_index(u, x, y, z)] = 0.0;
     return;
   }
-  const Offs nb = make_offs(g, x + u.ox, y + u.oy, z + u.oz);
+  const Nbr nb = make_nbr(g, x + u.ox, y + u.oy, z + u.oz, cell);
   int p;
   uint32_t c;
   state_slot(orient, d, m, cell, nb, p, c);
@@ -295,7 +312,7 @@ __global__ void unpack_plane_kernel(Grid g, UserBox u, int d, int orient,
 // density is 1 + sum g (the shift sums to 1, its first moment to 0).
 template <class ST>
 __device__ __forceinline__ void cell_moments(const Grid &g, const typename ST::S *state,
-    int orient, uint32_t m, uint32_t cell, const Offs &nb, float inv_scale, double &rho,
+    int orient, uint32_t m, uint32_t cell, const Nbr &nb, float inv_scale, double &rho,
     double &jx, double &jy, double &jz, bool &finite)
 {
   using V = typename ST::V;
@@ -326,11 +343,10 @@ __global__ void moments_kernel(Grid g, UserBox u, int orient, int quantity,
   const int x = blockIdx.z;
   if (z >= u.nz || y >= u.ny)
     return;
-  const uint32_t cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
-  const uint32_t m = mask[cell];
+  uint32_t cell, m;
   double r = 0.0;
-  if (!(m & kSolidBit)) {
-    const Offs nb = make_offs(g, x + u.ox, y + u.oy, z + u.oz);
+  if (locate(g, mask, x + u.ox, y + u.oy, z + u.oz, cell, m)) {
+    const Nbr nb = make_nbr(g, x + u.ox, y + u.oy, z + u.oz, cell);
     double rho, jx, jy, jz;
     bool fin;
     cell_moments<ST>(g, state, orient, m, cell, nb, inv_scale, rho, jx, jy, jz, fin);
@@ -379,11 +395,10 @@ __global__ void __launch_bounds__(kRedThreads) mass_kernel(Grid g, int orient,
     const long long r = i / g.nz;
     const int y = (int)(r % g.ny);
     const int x = (int)(r / g.ny);
-    const uint32_t cell = cell_index(g, x, y, z);
-    const uint32_t m = mask[cell];
-    if (m & kSolidBit)
+    uint32_t cell, m;
+    if (!locate(g, mask, x, y, z, cell, m))
       continue;
-    const Offs nb = make_offs(g, x, y, z);
+    const Nbr nb = make_nbr(g, x, y, z, cell);
     double rho, jx, jy, jz;
     bool fin;
     cell_moments<ST>(g, state, orient, m, cell, nb, inv_scale, rho, jx, jy, jz, fin);
@@ -425,11 +440,10 @@ __global__ void __launch_bounds__(kRedThreads) compare_kernel(Grid ga, Grid gb, 
     const long long r = i / ga.nz;
     const int y = (int)(r % ga.ny);
     const int x = (int)(r / ga.ny);
-    const uint32_t ca = cell_index(ga, x, y, z), cb = cell_index(gb, x, y, z);
-    const uint32_t ma = mask_a[ca], mb = mask_b[cb];
-    if ((ma & kSolidBit) || (mb & kSolidBit))
+    uint32_t ca, cb, ma, mb;
+    if (!locate(ga, mask_a, x, y, z, ca, ma) || !locate(gb, mask_b, x, y, z, cb, mb))
       continue;
-    const Offs na = make_offs(ga, x, y, z), nbb = make_offs(gb, x, y, z);
+    const Nbr na = make_nbr(ga, x, y, z, ca), nbb = make_nbr(gb, x, y, z, cb);
     double ra, xa, ya, za, rb, xb, yb, zb;
     bool fa, fb;
     cell_moments<SA>(ga, sa, oa, ma, ca, na, inv_a, ra, xa, ya, za, fa);
@@ -458,11 +472,10 @@ __global__ void __launch_bounds__(kRedThreads) outlet_kernel(Grid g, int x, int 
        i += (long long)gridDim.x * kRedThreads) {
     const int z = (int)(i % g.nz);
     const int y = (int)(i / g.nz);
-    const uint32_t cell = cell_index(g, x, y, z);
-    const uint32_t m = mask[cell];
-    if (m & kSolidBit)
+    uint32_t cell, m;
+    if (!locate(g, mask, x, y, z, cell, m))
       continue;
-    const Offs nb = make_offs(g, x, y, z);
+    const Nbr nb = make_nbr(g, x, y, z, cell);
     double rho, jx, jy, jz;
     bool fin;
     cell_moments<ST>(g, state, orient, m, cell, nb, inv_scale, rho, jx, jy, jz, fin);
@@ -501,6 +514,9 @@ static void free_all(lbm_solver *s)
   cudaFree(s->red);
   cudaFree(s->dev_err);
   cudaFree(s->bc_marks);
+  cudaFree(s->cbits);
+  cudaFree(s->cbase);
+  delete s->cplane0;
   free(s->split_done);
   if (s->fork_ev)
     cudaEventDestroy(s->fork_ev);
@@ -537,7 +553,8 @@ static int dev_alloc(lbm_solver *s, void **p, size_t bytes, const char *what)
 // slab = 1: flags has nx + 2 planes in x (x fastest); planes 0 and nx + 1
 // are the neighbouring slabs' boundary planes and become ghost planes.
 static int create_impl(lbm_solver **out, int nx, int ny, int nz, const int *flags,
-    int periodic_x, int periodic_y, int periodic_z, int pattern, int precision, int slab)
+    int periodic_x, int periodic_y, int periodic_z, int pattern, int precision, int slab,
+    int compact = 0)
 {
   if (!out)
     return fail(LBM_ERR_ARG, "lbm_create: out is NULL");
@@ -621,6 +638,48 @@ static int create_impl(lbm_solver **out, int nx, int ny, int nz, const int *flag
   }
   const long long pq = 256 / (long long)S;
   s->g.plane = (cells + pq - 1) / pq * pq;
+
+  // fluid bytes in device cell order (frames and padding = wall)
+  std::vector<uint8_t> fluid((size_t)cells, 0);
+  long long nf = 0;
+  for (int x = -slab; x < nx + slab; ++x)
+    for (int y = 0; y < ny; ++y)
+      for (int z = 0; z < nz; ++z) {
+        uint8_t f = flags[((long long)z * ny + y) * fx + x + slab] != 0;
+        fluid[((size_t)(x + frame[0]) * s->g.ny + (y + frame[1])) * s->g.pz + z + frame[2]] = f;
+        if (x >= 0 && x < nx)
+          nf += f;
+      }
+  s->n_fluid = nf;
+
+  // compact layout: one fluid bit per cell and the storage index of the
+  // first fluid cell of every 32-cell word, rows in (x, y) order
+  std::vector<uint32_t> hbits, hbase;
+  s->compact = compact && !slab;
+  if (s->compact) {
+    const int W = (s->g.nz + 31) / 32;
+    const size_t rows = (size_t)s->g.nx * s->g.ny;
+    hbits.assign(rows * W, 0u);
+    hbase.assign(rows * W, 0u);
+    uint32_t run = 0;
+    for (size_t r = 0; r < rows; ++r)
+      for (int w = 0; w < W; ++w) {
+        uint32_t bits = 0;
+        for (int b = 0; b < 32 && 32 * w + b < s->g.nz; ++b)
+          bits |= (uint32_t)fluid[r * s->g.pz + 32 * w + b] << b;
+        hbits[r * W + w] = bits;
+        hbase[r * W + w] = run;
+        run += (uint32_t)__builtin_popcount(bits);
+      }
+    s->g.W = W;
+    s->cplane0 = new std::vector<uint32_t>((size_t)s->g.nx + 1);
+    for (int x = 0; x < s->g.nx; ++x)
+      (*s->cplane0)[x] = hbase[(size_t)x * s->g.ny * W];
+    (*s->cplane0)[s->g.nx] = run;
+    s->g.plane = ((long long)run + pq - 1) / pq * pq;
+    if (s->g.plane == 0)
+      s->g.plane = pq;
+  }
   s->state_bytes = (size_t)Q * (size_t)s->g.plane * S;
 
 #define TRY(x)                                                                              \
@@ -677,7 +736,7 @@ static int create_impl(lbm_solver **out, int nx, int ny, int nz, const int *flag
     int optin = 0, sms = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
-    s->tma = precision == LBM_F64 && e && e[0] == '1' && optin > 1024 &&
+    s->tma = precision == LBM_F64 && !s->compact && e && e[0] == '1' && optin > 1024 &&
         tma_shape(s->g, storage_size(precision), env_int("LBM_B200_TMA_T"),
             env_int("LBM_B200_TMA_STAGES"), (size_t)optin - 1024, s->tma_shape);
     s->tma_groups = env_int("LBM_B200_TMA_GROUPS");
@@ -711,40 +770,57 @@ static int create_impl(lbm_solver **out, int nx, int ny, int nz, const int *flag
     }
   }
 
-  // fluid bytes in device cell order (frames and padding = wall), then the masks
-  std::vector<uint8_t> fluid((size_t)cells, 0);
-  long long nf = 0;
-  for (int x = -slab; x < nx + slab; ++x)
-    for (int y = 0; y < ny; ++y)
-      for (int z = 0; z < nz; ++z) {
-        uint8_t f = flags[((long long)z * ny + y) * fx + x + slab] != 0;
-        fluid[((size_t)(x + frame[0]) * s->g.ny + (y + frame[1])) * s->g.pz + z + frame[2]] = f;
-        if (x >= 0 && x < nx)
-          nf += f;
-      }
-  s->n_fluid = nf;
+  // the link masks: built on the dense cells, then (compact layout) moved to
+  // the fluid cells' storage indices
+  if (s->compact) {
+    const size_t nw = hbits.size() * sizeof(uint32_t);
+    TRY(dev_alloc(s, (void **)&s->cbits, nw, "the compact layout's fluid bits"));
+    TRY(dev_alloc(s, (void **)&s->cbase, nw, "the compact layout's word bases"));
+    TRYC(cudaMemcpy(s->cbits, hbits.data(), nw, cudaMemcpyHostToDevice));
+    TRYC(cudaMemcpy(s->cbase, hbase.data(), nw, cudaMemcpyHostToDevice));
+    s->g.bits = s->cbits;
+    s->g.base = s->cbase;
+  }
+  Grid gd = s->g; // dense view of the box for the mask build
+  gd.bits = nullptr;
+  gd.base = nullptr;
+  const long long dense_plane = (cells + pq - 1) / pq * pq;
+  uint32_t *dmask = s->mask;
+  if (s->compact)
+    TRYC(cudaMalloc((void **)&dmask, (size_t)dense_plane * 4));
   uint8_t *dfluid = NULL;
-  TRYC(cudaMalloc((void **)&dfluid, (size_t)cells));
-  cudaError_t e = cudaMemcpyAsync(dfluid, fluid.data(), (size_t)cells, cudaMemcpyHostToDevice,
-      s->stream);
+  cudaError_t e = cudaMalloc((void **)&dfluid, (size_t)cells);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dfluid, fluid.data(), (size_t)cells, cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess) {
-    Grid gp = s->g;
+    Grid gp = gd;
     gp.nz = s->g.pz; // cover the row padding too
     dim3 grid, block;
     cell_launch_shape(gp, grid, block);
-    mask_kernel<<<grid, block, 0, s->stream>>>(s->g, dfluid, s->mask, s->slab);
+    mask_kernel<<<grid, block, 0, s->stream>>>(gd, dfluid, dmask, s->slab);
     e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && s->compact) {
+    e = cudaMemsetAsync(s->mask, 0xFF, (size_t)s->g.plane * 4, s->stream); // unused: walls
+    dim3 grid, block;
+    cell_launch_shape(s->g, grid, block);
+    if (e == cudaSuccess)
+      compact_mask_kernel<<<grid, block, 0, s->stream>>>(s->g, dmask, s->mask);
+    if (e == cudaSuccess)
+      e = cudaGetLastError();
   }
   if (e == cudaSuccess)
     e = cudaStreamSynchronize(s->stream);
   cudaFree(dfluid);
+  if (s->compact)
+    cudaFree(dmask);
   if (e != cudaSuccess) {
     free_all(s);
     return fail(LBM_ERR_CUDA, "lbm_create: mask build failed: %s", cudaGetErrorString(e));
   }
   // cells beyond the box inside the rounded plane stay unused; mark them as
   // walls so no kernel that walks the whole plane treats them as fluid
-  if (s->g.plane > cells) {
+  if (!s->compact && s->g.plane > cells) {
     std::vector<uint32_t> pad((size_t)(s->g.plane - cells), kSolidBit);
     TRYC(cudaMemcpy(s->mask + cells, pad.data(), pad.size() * 4, cudaMemcpyHostToDevice));
   }
@@ -760,6 +836,15 @@ extern "C" int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *f
   return create_impl(out, nx, ny, nz, flags, periodic_x, periodic_y, periodic_z, pattern,
       precision, 0);
 }
+
+extern "C" int lbm_create_compact(lbm_solver **out, int nx, int ny, int nz, const int *flags,
+    int periodic_x, int periodic_y, int periodic_z, int pattern, int precision)
+{
+  return create_impl(out, nx, ny, nz, flags, periodic_x, periodic_y, periodic_z, pattern,
+      precision, 0, 1);
+}
+
+extern "C" int lbm_is_compact(const lbm_solver *s) { return s ? s->compact : -1; }
 
 extern "C" int lbm_create_slab(lbm_solver **out, int nx, int ny, int nz, const int *flags,
     int periodic_y, int periodic_z, int pattern, int precision)
@@ -805,6 +890,9 @@ extern "C" int lbm_set_fp16_scale(lbm_solver *s, double scale)
 
 extern "C" int lbm_set_porosity(lbm_solver *s, const float *porosity, double alpha)
 {
+  if (s && s->compact)
+    return fail(LBM_ERR_ARG, "lbm_set_porosity: the compact layout has no Brinkman term "
+        "(use lbm_create)");
   if (!s)
     return fail(LBM_ERR_ARG, "lbm_set_porosity: NULL solver");
   if (alpha == 0.0) {
@@ -941,12 +1029,11 @@ __global__ void pack_ref_kernel(Grid g, UserBox u, int p, int ref_orient, int or
   const int x = blockIdx.z;
   if (z >= u.nz || y >= u.ny)
     return;
-  const uint32_t cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
-  const uint32_t m = mask[cell];
-  if (m & kSolidBit)
+  uint32_t cell, m;
+  if (!locate(g, mask, x + u.ox, y + u.oy, z + u.oz, cell, m))
     return;
   const int d = (ref_orient == LBM_REF_AA_EVEN) ? inv(p) : p;
-  const Offs nb = make_offs(g, x + u.ox, y + u.oy, z + u.oz);
+  const Nbr nb = make_nbr(g, x + u.ox, y + u.oy, z + u.oz, cell);
   int sp;
   uint32_t sc;
   state_slot(orient, d, m, cell, nb, sp, sc);
@@ -969,12 +1056,11 @@ __global__ void unpack_ref_kernel(Grid g, UserBox u, int p, int ref_orient, int 
   const int x = blockIdx.z;
   if (z >= u.nz || y >= u.ny)
     return;
-  const uint32_t cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
-  const uint32_t m = mask[cell];
-  if (m & kSolidBit)
+  uint32_t cell, m;
+  if (!locate(g, mask, x + u.ox, y + u.oy, z + u.oz, cell, m))
     return;
   const int d = (ref_orient == LBM_REF_AA_EVEN) ? inv(p) : p;
-  const Offs nb = make_offs(g, x + u.ox, y + u.oy, z + u.oz);
+  const Nbr nb = make_nbr(g, x + u.ox, y + u.oy, z + u.oz, cell);
   int sp;
   uint32_t sc;
   state_slot(orient, d, m, cell, nb, sp, sc);
@@ -1014,17 +1100,14 @@ __global__ void aos_ref_kernel(Grid g, UserBox u, int a0, int ref_orient, int or
     }
     bool own = x >= 0 && x < u.nx && y >= 0 && y < u.ny && z >= 0 && z < u.nz;
     uint32_t cell = 0, m = kSolidBit;
-    if (own) {
-      cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
-      m = mask[cell];
-      own = !(m & kSolidBit);
-    }
+    if (own)
+      own = locate(g, mask, x + u.ox, y + u.oy, z + u.oz, cell, m);
     if (!own) {
       if (!UP)
         slots[p] = (H)0;
       continue;
     }
-    const Offs nb = make_offs(g, x + u.ox, y + u.oy, z + u.oz);
+    const Nbr nb = make_nbr(g, x + u.ox, y + u.oy, z + u.oz, cell);
     int sp;
     uint32_t sc;
     state_slot(orient, d, m, cell, nb, sp, sc);
@@ -1189,7 +1272,49 @@ static int launch_kernel(lbm_solver *s, int x0, int planes, cudaStream_t st, int
   const bool brink = s->alpha != 0.0 && s->porosity;
   const bool force = s->force_on || brink;
   cudaError_t e;
-  if (s->precision == LBM_F64) {
+  if (s->compact) {
+    // compact layout: one cell per thread in every precision (no Brinkman term)
+    if (s->precision == LBM_F64) {
+      StepArgs<StoreF64> a;
+      a.g = s->g;
+      a.src = (const double *)src;
+      a.dst = (double *)dst;
+      a.mask = s->mask;
+      a.porosity = nullptr;
+      a.u_save = nullptr;
+      a.c = make_consts<double>(s);
+      a.x0 = x0;
+      a.c0 = (*s->cplane0)[x0];
+      a.cn = (*s->cplane0)[x0 + planes] - a.c0;
+      e = launch_step_cp_f64(kind, force, a, grid, block, st);
+    } else if (s->precision == LBM_F32) {
+      StepArgs<StoreF32> a;
+      a.g = s->g;
+      a.src = (const float *)src;
+      a.dst = (float *)dst;
+      a.mask = s->mask;
+      a.porosity = nullptr;
+      a.u_save = nullptr;
+      a.c = make_consts<float>(s);
+      a.x0 = x0;
+      a.c0 = (*s->cplane0)[x0];
+      a.cn = (*s->cplane0)[x0 + planes] - a.c0;
+      e = launch_step_cp_f32(kind, force, a, grid, block, st);
+    } else {
+      StepArgs<StoreF16> a;
+      a.g = s->g;
+      a.src = (const __half *)src;
+      a.dst = (__half *)dst;
+      a.mask = s->mask;
+      a.porosity = nullptr;
+      a.u_save = nullptr;
+      a.c = make_consts<float>(s);
+      a.x0 = x0;
+      a.c0 = (*s->cplane0)[x0];
+      a.cn = (*s->cplane0)[x0 + planes] - a.c0;
+      e = launch_step_cp_f16(kind, force, a, grid, block, st);
+    }
+  } else if (s->precision == LBM_F64) {
     StepArgs<StoreF64> a;
     a.g = s->g;
     a.src = (const double *)src;
@@ -1839,9 +1964,8 @@ __global__ void init_equilibrium_kernel(Grid g, UserBox u, int orient, typename 
   const int x = blockIdx.z;
   if (z >= u.nz || y >= u.ny)
     return;
-  const uint32_t cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
-  const uint32_t m = mask[cell];
-  if (m & kSolidBit)
+  uint32_t cell, m;
+  if (!locate(g, mask, x + u.ox, y + u.oy, z + u.oz, cell, m))
     return;
   const long long c = dense_index(u, x, y, z);
   uint64_t st = (uint64_t)seed ^ mix64_d((uint64_t)c * 0x9E3779B97F4A7C15ull + 1ull);
@@ -1855,7 +1979,7 @@ __global__ void init_equilibrium_kernel(Grid g, UserBox u, int orient, typename 
   }
   const double usq = __dadd_rn(__dadd_rn(__dmul_rn(uu[0], uu[0]), __dmul_rn(uu[1], uu[1])),
       __dmul_rn(uu[2], uu[2]));
-  const Offs nb = make_offs(g, x + u.ox, y + u.oy, z + u.oz);
+  const Nbr nb = make_nbr(g, x + u.ox, y + u.oy, z + u.oz, cell);
 #pragma unroll
   for (int d = 0; d < Q; ++d) {
     const int wc = wclass(d);

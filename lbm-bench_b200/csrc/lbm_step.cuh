@@ -53,6 +53,7 @@ template <class ST> struct StepArgs {
   V *u_save;             // Brinkman only, optional: momentum per cell (3 planes)
   Consts<V> c;
   int x0 = 0;            // first storage x plane of the launch (grid.z planes from there)
+  uint32_t c0 = 0, cn = 0; // compact layout, local steps: storage indices [c0, c0 + cn)
 };
 
 // Minimum resident blocks per SM requested from the compiler (caps the

@@ -1,0 +1,252 @@
+// Step kernels of the compact (fluid-only) layout: the same fused
+// stream-collide-bounce-back(-force) step as step_kernel (lbm_step.cuh,
+// whose header gives the per-pattern read and write rules and the
+// bit-exactness argument), with every population plane and the link masks
+// holding fluid cells only, in row order (Grid, lbm_device.cuh).
+//
+// The dense layout stores every cell, and a 128-byte line that holds both
+// fluid and solid cells is fetched whole from HBM: in a 20%-solid porous
+// channel that is 14% (FP64) to 26% (FP16) more DRAM traffic than the
+// algorithmic 2 x 19 x S bytes per fluid update. The reference sweeps the
+// dense box too (src/kernel_pull_soa.c:94-96). Here no solid cell occupies
+// storage, so every fetched sector belongs to fluid cells.
+//
+// Threads still map to device cells - z across the lanes, one warp per 32
+// consecutive z of one (x, y) row, starting at a multiple of 32 - and a
+// solid lane leaves after one fluid-bit test. Because a warp's lanes share
+// the row and the fluid-bit word, the storage index of a fluid cell and of
+// its neighbours comes from nine warp-uniform word pairs (own row and the
+// eight rows (x +- 1, y +- 1)): with B_q = base + popc(word_q & bits below
+// z) and f_q the fluid bit of (row q, z),
+//     index of (row q, z)     = B_q
+//     index of (row q, z + 1) = B_q + f_q      (when that cell is fluid)
+//     index of (row q, z - 1) = B_q - 1        (when that cell is fluid)
+// which also holds across word boundaries (base of word w + 1 is base of
+// word w plus its popcount). Only a periodic z axis breaks it at z = 0 and
+// z = nz - 1; those lanes look the wrapped neighbour up directly. Whether a
+// neighbour is fluid comes from the cell's link mask, as in the dense
+// kernel, so a wall neighbour never needs an index.
+#pragma once
+
+#include "lbm_step.cuh"
+
+namespace lbm {
+
+// Register caps of the compact kernels (minimum CTAs per SM), per kind from
+// a sweep on the 256^3 porous channel (B200): AA odd and pull are fastest
+// at 8 CTAs/SM (64 registers; odd 0.963 ms at 6 with the row table in
+// registers, 0.803 at 6 and 0.764 at 8 with it in shared memory), push at 7,
+// the local AA even step (at the HBM limit) does not care.
+#ifndef LBM_MINB_CP_ODD
+#define LBM_MINB_CP_ODD 8
+#endif
+#ifndef LBM_MINB_CP_PULL
+#define LBM_MINB_CP_PULL 8
+#endif
+#ifndef LBM_MINB_CP_PUSH
+#define LBM_MINB_CP_PUSH 7
+#endif
+#ifndef LBM_MINB_CP_EVEN
+#define LBM_MINB_CP_EVEN 6
+#endif
+template <int KIND> struct CpOccupancy {
+  static constexpr int value = KIND == kAAEvenStep ? LBM_MINB_CP_EVEN
+      : KIND == kAAOddStep ? LBM_MINB_CP_ODD
+      : KIND == kPullStep ? LBM_MINB_CP_PULL : LBM_MINB_CP_PUSH;
+};
+
+// Storage indices of the 18 neighbours of one fluid cell (compact layout).
+// Kernels that scatter (push, AA odd) need them again after the collision;
+// they keep them in shared memory (one column per thread) rather than in
+// registers across it. Entry q = (dx + 1) * 3 + (dy + 1) (q != 4) holds B_q,
+// the index of (x + dx, y + dy, z) or of the next fluid z; entries 9..12
+// hold B_q + f_q for the four axis rows q = 1, 3, 5, 7, the index of
+// (row q, z + 1). ZPER: the z axis is periodic, and lanes on z = 0 or
+// z = nz - 1 look their wrapped z neighbours up directly.
+#ifndef LBM_CP_SMEM_TAB
+#define LBM_CP_SMEM_TAB 1
+#endif
+constexpr int kTabRows = 13;
+
+template <bool ZPER> struct RowTab {
+  uint32_t B[kTabRows];
+  uint32_t *sB = nullptr; // shared copy: sB[k * kStepThreads]
+  bool zwrap = false;
+  int x, y, z;
+
+  __device__ __forceinline__ static int axis_slot(int q)
+  {
+    return q == 1 ? 9 : q == 3 ? 10 : q == 5 ? 11 : 12;
+  }
+
+  __device__ __forceinline__ void build(const Grid &g, int x_, int y_, int z_, uint32_t cell,
+      uint32_t wi, uint32_t lt, int lane)
+  {
+    x = x_;
+    y = y_;
+    z = z_;
+    B[4] = cell;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      if (q == 4)
+        continue;
+      int xr = x + q / 3 - 1, yr = y + q % 3 - 1;
+      // out-of-range rows only occur on non-periodic faces, whose cells are
+      // walls (the mask says so and the index is never used): wrap anyway
+      xr = xr < 0 ? g.nx - 1 : xr >= g.nx ? 0 : xr;
+      yr = yr < 0 ? g.ny - 1 : yr >= g.ny ? 0 : yr;
+      const uint32_t k = ((uint32_t)xr * (uint32_t)g.ny + (uint32_t)yr) * (uint32_t)g.W + wi;
+      const uint32_t w = __ldg(g.bits + k);
+      B[q] = __ldg(g.base + k) + (uint32_t)__popc(w & lt);
+      if (q == 1 || q == 3 || q == 5 || q == 7)
+        B[axis_slot(q)] = B[q] + ((w >> lane) & 1u);
+    }
+    if (sB) {
+#pragma unroll
+      for (int k = 0; k < kTabRows; ++k)
+        if (k != 4)
+          sB[k * kStepThreads] = B[k];
+    }
+    if (ZPER)
+      zwrap = z == 0 || z == g.nz - 1;
+  }
+
+  __device__ __forceinline__ uint32_t entry(int k) const
+  {
+    return (sB && k != 4) ? sB[k * kStepThreads] : B[k];
+  }
+
+  // storage index of x + c_d; meaningful only when that cell is fluid
+  __device__ __forceinline__ uint32_t at(const Grid &g, int d) const
+  {
+    const int q = (cx(d) + 1) * 3 + (cy(d) + 1);
+    if (ZPER && cz(d) != 0 && zwrap) {
+      int a = x + cx(d), b = y + cy(d), c = z + cz(d);
+      a = a < 0 ? g.nx - 1 : a >= g.nx ? 0 : a;
+      b = b < 0 ? g.ny - 1 : b >= g.ny ? 0 : b;
+      c = c < 0 ? g.nz - 1 : c >= g.nz ? 0 : c;
+      return packed_index(g, a, b, c);
+    }
+    if (cz(d) > 0)
+      return q == 4 ? B[4] + 1u : entry(axis_slot(q));
+    if (cz(d) < 0)
+      return entry(q) - 1u;
+    return entry(q);
+  }
+};
+
+// OFF: type of element offsets within the state (uint32_t when all 19
+// planes fit below 2^32 elements, which keeps address arithmetic 32-bit).
+template <class ST, int KIND, bool FORCE, bool ZPER, typename OFF>
+__global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND>::value))
+    step_kernel_cp(StepArgs<ST> a)
+{
+  using S = typename ST::S;
+  using V = typename ST::V;
+  constexpr bool kNC = (KIND == kPullStep || KIND == kPushStep);
+  const Grid &g = a.g;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = a.x0 + (int)blockIdx.z;
+  if (z >= g.nz || y >= g.ny)
+    return;
+  const int lane = z & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t wi = (uint32_t)(z >> 5);
+  const uint32_t k0 = ((uint32_t)x * (uint32_t)g.ny + (uint32_t)y) * (uint32_t)g.W + wi;
+  const uint32_t w0 = __ldg(g.bits + k0);
+  if (!((w0 >> lane) & 1u))
+    return;
+  const uint32_t cell = __ldg(g.base + k0) + (uint32_t)__popc(w0 & lt);
+  const uint32_t mask = __ldg(a.mask + cell);
+  const S *src = a.src;
+  S *dst = a.dst;
+  const OFF P = (OFF)g.plane;
+  auto el = [&](int plane, uint32_t i) { return (OFF)plane * P + (OFF)i; };
+
+  RowTab<ZPER> t;
+  constexpr bool kScatter = (KIND == kPushStep || KIND == kAAOddStep);
+  if (kScatter && LBM_CP_SMEM_TAB) {
+    __shared__ uint32_t tab[kTabRows * kStepThreads];
+    t.sB = tab + (threadIdx.y * blockDim.x + threadIdx.x);
+  }
+  if (KIND != kAAEvenStep)
+    t.build(g, x, y, z, cell, wi, lt, lane);
+
+  V f[Q];
+  if (KIND == kPushStep || KIND == kAAEvenStep) {
+    // local loads: issued without waiting for the mask
+#pragma unroll
+    for (int d = 0; d < Q; ++d)
+      f[d] = ST::decode(ldg<kNC>(src + el(d, cell)), a.c.inv_scale);
+  } else if (!__any_sync(__activemask(), (mask & 0x7FFFFu) != 0u)) {
+    // no lane of the warp has a wall link: no redirects
+#pragma unroll
+    for (int d = 0; d < Q; ++d) {
+      const OFF o = (KIND == kPullStep) ? el(d, t.at(g, inv(d))) : el(inv(d), t.at(g, inv(d)));
+      f[d] = ST::decode(ldg<kNC>(src + o), a.c.inv_scale);
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < Q; ++d) {
+      const bool back = (mask >> inv(d)) & 1u;
+      OFF o;
+      if (KIND == kPullStep)
+        o = back ? el(inv(d), cell) : el(d, t.at(g, inv(d)));
+      else
+        o = back ? el(d, cell) : el(inv(d), t.at(g, inv(d)));
+      f[d] = ST::decode(ldg<kNC>(src + o), a.c.inv_scale);
+    }
+  }
+
+  V o[Q];
+  collide<V, false>(f, o, a.c, V(0));
+
+#pragma unroll
+  for (int d = 0; d < Q; ++d) {
+    const bool bb = (mask >> d) & 1u;
+    const V v = FORCE ? o[d] + (bb ? a.c.force[inv(d)] : a.c.force[d]) : o[d];
+    OFF off;
+    if (KIND == kPullStep)
+      off = el(d, cell);
+    else if (KIND == kAAEvenStep)
+      off = el(inv(d), cell);
+    else
+      off = bb ? el(inv(d), cell) : el(d, t.at(g, d));
+    dst[off] = ST::encode(v, a.c.scale);
+  }
+}
+
+// The AA even step in the compact layout is local - a cell reads and writes
+// only its own 19 slots - so threads map straight to storage indices: thread
+// i updates cell c0 + i, a warp touches 32 consecutive elements of every
+// plane, and the mask and population loads are issued together with no
+// index lookup in front of them. Only the link mask (bounce-back force
+// direction) is read besides the populations.
+template <class ST, bool FORCE>
+__global__ void __launch_bounds__(kStepThreads, (CpOccupancy<kAAEvenStep>::value))
+    step_kernel_cp_local(StepArgs<ST> a)
+{
+  using S = typename ST::S;
+  using V = typename ST::V;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.cn)
+    return;
+  const uint32_t cell = a.c0 + i;
+  const uint32_t mask = __ldg(a.mask + cell);
+  const long long P = a.g.plane;
+  V f[Q];
+#pragma unroll
+  for (int d = 0; d < Q; ++d)
+    f[d] = ST::decode(a.src[d * P + cell], a.c.inv_scale);
+  V o[Q];
+  collide<V, false>(f, o, a.c, V(0));
+#pragma unroll
+  for (int d = 0; d < Q; ++d) {
+    const bool bb = (mask >> d) & 1u;
+    const V v = FORCE ? o[d] + (bb ? a.c.force[inv(d)] : a.c.force[d]) : o[d];
+    a.dst[inv(d) * P + cell] = ST::encode(v, a.c.scale);
+  }
+}
+
+} // namespace lbm

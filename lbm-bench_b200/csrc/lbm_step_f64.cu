@@ -94,11 +94,10 @@ __global__ void pressure_bc_kernel(Grid g, UserBox u, int orient, typename ST::S
   if (z >= u.nz || y >= u.ny || !marks[((size_t)side * u.ny + y) * u.nz + z])
     return;
   const int x = side ? u.nx - 1 : 0;
-  const uint32_t cell = cell_index(g, x + u.ox, y + u.oy, z + u.oz);
-  const uint32_t m = mask[cell];
-  if (m & kSolidBit)
+  uint32_t cell, m;
+  if (!locate(g, mask, x + u.ox, y + u.oy, z + u.oz, cell, m))
     return;
-  const Offs nb = make_offs(g, x + u.ox, y + u.oy, z + u.oz);
+  const Nbr nb = make_nbr(g, x + u.ox, y + u.oy, z + u.oz, cell);
   auto at = [&](int d) {
     int p;
     uint32_t c;
@@ -176,6 +175,59 @@ cudaError_t launch_step_f64(int kind, bool force, bool brink, const StepArgs<Sto
   case kAAOddStep: return pick<kAAOddStep>(force, brink, a, grid, block, st);
   }
   return cudaErrorInvalidValue;
+}
+
+template <class ST, int KIND>
+static cudaError_t go_cp(bool force, const StepArgs<ST> &a, dim3 grid, dim3 block,
+    cudaStream_t st)
+{
+  if (KIND == kAAEvenStep) {
+    if (a.cn == 0)
+      return cudaSuccess;
+    const unsigned nb = (a.cn + kStepThreads - 1) / kStepThreads;
+    if (force)
+      step_kernel_cp_local<ST, true><<<nb, kStepThreads, 0, st>>>(a);
+    else
+      step_kernel_cp_local<ST, false><<<nb, kStepThreads, 0, st>>>(a);
+    return cudaGetLastError();
+  }
+  const bool zper = (a.g.per & 4) != 0;
+  const bool off32 = (unsigned long long)Q * (unsigned long long)a.g.plane < (1ull << 32);
+  if (off32) {
+    if (force)
+      zper ? step_kernel_cp<ST, KIND, true, true, uint32_t><<<grid, block, 0, st>>>(a)
+           : step_kernel_cp<ST, KIND, true, false, uint32_t><<<grid, block, 0, st>>>(a);
+    else
+      zper ? step_kernel_cp<ST, KIND, false, true, uint32_t><<<grid, block, 0, st>>>(a)
+           : step_kernel_cp<ST, KIND, false, false, uint32_t><<<grid, block, 0, st>>>(a);
+  } else {
+    if (force)
+      zper ? step_kernel_cp<ST, KIND, true, true, uint64_t><<<grid, block, 0, st>>>(a)
+           : step_kernel_cp<ST, KIND, true, false, uint64_t><<<grid, block, 0, st>>>(a);
+    else
+      zper ? step_kernel_cp<ST, KIND, false, true, uint64_t><<<grid, block, 0, st>>>(a)
+           : step_kernel_cp<ST, KIND, false, false, uint64_t><<<grid, block, 0, st>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+template <class ST>
+static cudaError_t launch_cp(int kind, bool force, const StepArgs<ST> &a, dim3 grid, dim3 block,
+    cudaStream_t st)
+{
+  switch (kind) {
+  case kPullStep: return go_cp<ST, kPullStep>(force, a, grid, block, st);
+  case kPushStep: return go_cp<ST, kPushStep>(force, a, grid, block, st);
+  case kAAEvenStep: return go_cp<ST, kAAEvenStep>(force, a, grid, block, st);
+  case kAAOddStep: return go_cp<ST, kAAOddStep>(force, a, grid, block, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_step_cp_f64(int kind, bool force, const StepArgs<StoreF64> &a, dim3 grid,
+    dim3 block, cudaStream_t st)
+{
+  return launch_cp<StoreF64>(kind, force, a, grid, block, st);
 }
 
 } // namespace lbm

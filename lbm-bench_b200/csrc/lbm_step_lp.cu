@@ -86,4 +86,63 @@ cudaError_t launch_step_x2_f16(int kind, bool force, bool brink, const StepArgs2
   return launch(kind, force, brink, a, st);
 }
 
+template <class ST, int KIND>
+static cudaError_t go_cp(bool force, const StepArgs<ST> &a, dim3 grid, dim3 block,
+    cudaStream_t st)
+{
+  if (KIND == kAAEvenStep) {
+    if (a.cn == 0)
+      return cudaSuccess;
+    const unsigned nb = (a.cn + kStepThreads - 1) / kStepThreads;
+    if (force)
+      step_kernel_cp_local<ST, true><<<nb, kStepThreads, 0, st>>>(a);
+    else
+      step_kernel_cp_local<ST, false><<<nb, kStepThreads, 0, st>>>(a);
+    return cudaGetLastError();
+  }
+  const bool zper = (a.g.per & 4) != 0;
+  const bool off32 = (unsigned long long)Q * (unsigned long long)a.g.plane < (1ull << 32);
+  if (off32) {
+    if (force)
+      zper ? step_kernel_cp<ST, KIND, true, true, uint32_t><<<grid, block, 0, st>>>(a)
+           : step_kernel_cp<ST, KIND, true, false, uint32_t><<<grid, block, 0, st>>>(a);
+    else
+      zper ? step_kernel_cp<ST, KIND, false, true, uint32_t><<<grid, block, 0, st>>>(a)
+           : step_kernel_cp<ST, KIND, false, false, uint32_t><<<grid, block, 0, st>>>(a);
+  } else {
+    if (force)
+      zper ? step_kernel_cp<ST, KIND, true, true, uint64_t><<<grid, block, 0, st>>>(a)
+           : step_kernel_cp<ST, KIND, true, false, uint64_t><<<grid, block, 0, st>>>(a);
+    else
+      zper ? step_kernel_cp<ST, KIND, false, true, uint64_t><<<grid, block, 0, st>>>(a)
+           : step_kernel_cp<ST, KIND, false, false, uint64_t><<<grid, block, 0, st>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+template <class ST>
+static cudaError_t launch_cp(int kind, bool force, const StepArgs<ST> &a, dim3 grid, dim3 block,
+    cudaStream_t st)
+{
+  switch (kind) {
+  case kPullStep: return go_cp<ST, kPullStep>(force, a, grid, block, st);
+  case kPushStep: return go_cp<ST, kPushStep>(force, a, grid, block, st);
+  case kAAEvenStep: return go_cp<ST, kAAEvenStep>(force, a, grid, block, st);
+  case kAAOddStep: return go_cp<ST, kAAOddStep>(force, a, grid, block, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_step_cp_f32(int kind, bool force, const StepArgs<StoreF32> &a, dim3 grid,
+    dim3 block, cudaStream_t st)
+{
+  return launch_cp<StoreF32>(kind, force, a, grid, block, st);
+}
+
+cudaError_t launch_step_cp_f16(int kind, bool force, const StepArgs<StoreF16> &a, dim3 grid,
+    dim3 block, cudaStream_t st)
+{
+  return launch_cp<StoreF16>(kind, force, a, grid, block, st);
+}
+
 } // namespace lbm

@@ -40,6 +40,21 @@ static int body_force_on(void)
   return e && e[0] == '1';
 }
 
+/* Storage layout of the drop-in solvers: the compact (fluid-only) layout
+ * for FP64, where it is faster for every pattern, and the dense layout for
+ * the reduced-precision names, whose multi-cell kernels are written for it.
+ * The environment variable LBM_B200_LAYOUT=dense or =compact overrides the
+ * choice; results are the same either way (FP64 bit for bit). */
+static int use_compact(int precision)
+{
+  const char *e = getenv("LBM_B200_LAYOUT");
+  if (e && strcmp(e, "dense") == 0)
+    return 0;
+  if (e && strcmp(e, "compact") == 0)
+    return 1;
+  return precision == LBM_F64;
+}
+
 static void die(const char *what)
 {
   printf("ERROR: %s: %s\n", what, lbm_last_error());
@@ -248,12 +263,15 @@ static void initCuda(LatticeDescType *ld, KernelDataType **kdp, int pattern, int
     kd->BoundaryConditionsSetPdf = bcSetAa;
   }
   kd->Kernel = cudaKernel;
-  if (lbm_create(&ck->solver, ld->Dims[0], ld->Dims[1], ld->Dims[2], ld->Lattice, ld->PeriodicX,
-          ld->PeriodicY, ld->PeriodicZ, pattern, precision) != LBM_OK)
+  const int compact = use_compact(precision);
+  if ((compact ? lbm_create_compact : lbm_create)(&ck->solver, ld->Dims[0], ld->Dims[1],
+          ld->Dims[2], ld->Lattice, ld->PeriodicX, ld->PeriodicY, ld->PeriodicZ, pattern,
+          precision) != LBM_OK)
     die(name);
-  printf("# %s: %lld LB nodes with padding, host %.1f MiB (%s), device %.1f MiB\n", name,
-      cells, nbuf * ck->pdf_bytes / 1048576.0, nbuf == 1 ? "single lattice" : "both lattices",
-      lbm_device_bytes(ck->solver) / 1048576.0);
+  printf("# %s: %lld LB nodes with padding, host %.1f MiB (%s), device %.1f MiB (%s layout)\n",
+      name, cells, nbuf * ck->pdf_bytes / 1048576.0,
+      nbuf == 1 ? "single lattice" : "both lattices", lbm_device_bytes(ck->solver) / 1048576.0,
+      compact ? "compact" : "dense");
   printf("# bounce-back PDFs: %d\n", kd->nBounceBackPdfs);
   if (host_layout == HOST_BLK)
     printf("# blocking x: %3d y: %3d z: %3d\n", kd->Blk[0], kd->Blk[1], kd->Blk[2]);

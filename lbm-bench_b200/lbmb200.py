@@ -47,6 +47,10 @@ _SIGNATURES = [
     ("lbm_create", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                   _ip, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_int]),
+    ("lbm_create_compact", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    ("lbm_is_compact", ctypes.c_int, [_vp]),
     ("lbm_create_slab", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, ctypes.c_int]),
@@ -149,7 +153,8 @@ def _addr(buf) -> int:
 class Solver:
     """One device lattice (include/lbm_b200.h lbm_create ... lbm_destroy)."""
 
-    def __init__(self, flags, periodic=(1, 0, 0), pattern=AA, precision=F64):
+    def __init__(self, flags, periodic=(1, 0, 0), pattern=AA, precision=F64, compact=False):
+        """compact=True: the fluid-only layout (lbm_create_compact)."""
         if isinstance(pattern, str):
             pattern = PATTERNS[pattern]
         if isinstance(precision, str):
@@ -161,9 +166,14 @@ class Solver:
         self.pattern, self.precision = pattern, precision
         self.periodic = tuple(int(p) for p in periodic)
         h = _vp()
-        _check(lib().lbm_create(ctypes.byref(h), nx, ny, nz, _p(flags, _ip), *self.periodic,
-                                pattern, precision))
+        create = lib().lbm_create_compact if compact else lib().lbm_create
+        _check(create(ctypes.byref(h), nx, ny, nz, _p(flags, _ip), *self.periodic, pattern,
+                      precision))
         self._h = h
+
+    @property
+    def compact(self) -> bool:
+        return lib().lbm_is_compact(self._h) == 1
 
     @classmethod
     def slab(cls, flags, periodic_yz=(0, 0), pattern=AA, precision=F64):
