@@ -330,22 +330,22 @@ def run_native(args, dist: Dist):
             "layout": "compact" if cp else "dense", "device_bytes": v.device_bytes}
         variants[key]["frac"] = variants[key]["gbs"] / peak
         v.close()
-    # FP32 / FP16 storage in the dense layout (its multi-cell kernels are faster there)
+    # FP32 / FP16 storage in both layouts (bit-identical results)
     ref = solver(L, flags, "aa", L.F64, f0, compact)  # accuracy reference: FP64, same seed
     ref.run(args.steps)
     for name, prec in (("fp32", L.F32), ("fp16", L.F16)):
-        for pattern in ("aa", "pull"):
-            b = solver(L, flags, pattern, prec, f0)
+        for pattern, cp in (("aa", False), ("pull", False), ("aa", True), ("pull", True)):
+            b = solver(L, flags, pattern, prec, f0, cp)
             b.run(args.warmup)
             t = b.run_timed(args.steps - args.warmup) if args.steps > args.warmup else None
             d = b.compare(ref)
             mlups = n_fluid * (args.steps - args.warmup) / (t / 1e3) / 1e6 if t else None
-            key = f"{name}_{pattern}"
+            key = f"{name}_{pattern}" + ("_compact" if cp else "")
             variants[key] = {
                 "mlups": mlups, "gbs": mlups * b.bytes_per_update / 1e3 if mlups else None,
                 "l2_rel_err_u": float(np.sqrt(d[0] / d[1])) if d[1] > 0 else None,
                 "l2_rel_err_rho": float(np.sqrt(d[2] / d[3])) if d[3] > 0 else None,
-                "error_after_steps": args.steps, "layout": "dense"}
+                "error_after_steps": args.steps, "layout": "compact" if cp else "dense"}
             if mlups:
                 variants[key]["frac"] = variants[key]["gbs"] / peak
                 variants[key]["speedup_vs_fp64_aa"] = mlups / (value / dist.world)
@@ -410,7 +410,8 @@ def summary(r):
               "fp64_aa_compact", "fp64_pull_compact", "fp64_push_compact"):
         if k in v:
             out[k] = {"mlups": _r(v[k]["mlups"]), "frac": _r(v[k]["frac"])}
-    for k in ("fp32_aa", "fp32_pull", "fp16_aa", "fp16_pull"):
+    for k in ("fp32_aa", "fp32_pull", "fp16_aa", "fp16_pull", "fp32_aa_compact",
+              "fp32_pull_compact", "fp16_aa_compact", "fp16_pull_compact"):
         if k in v and v[k]["mlups"]:
             out[k] = {"mlups": _r(v[k]["mlups"]), "frac": _r(v[k]["frac"]),
                       "x_fp64_aa": _r(v[k]["speedup_vs_fp64_aa"], 3),
@@ -419,17 +420,18 @@ def summary(r):
     if p:
         out["p512"] = {"fp64_aa": _r(p["fp64_aa"]["mlups"]),
                        "fp64_aa_dense": _r(p["fp64_aa_dense"]["mlups"])}
-        for k in ("fp32_aa", "fp16_aa"):
+        for k in ("fp32_aa", "fp16_aa", "fp32_aa_compact", "fp16_aa_compact"):
             out["p512"][k] = {"mlups": _r(p[k]["mlups"]), "frac": _r(p[k]["frac"]),
                               "x_fp64_aa": _r(p[k]["speedup_vs_fp64_aa"], 3),
                               "err_u": _r(p[k]["l2_rel_err_u"], 2),
                               "err_rho": _r(p[k]["l2_rel_err_rho"], 2)}
     g = r.get("largest")
     if g:
-        f = g["forward_fp16_aa"]
         a = g["adjoint"]["fp32"]
-        out["l768_fp16_aa"] = {"mlups": _r(f["mlups"]), "frac": _r(f["frac"]),
-                               "device_gb": _r(f["device_used_bytes"] / 1e9, 3)}
+        for k in ("forward_fp16_aa", "forward_fp16_aa_compact"):
+            f = g[k]
+            out["l768_" + k[8:]] = {"mlups": _r(f["mlups"]), "frac": _r(f["frac"]),
+                                     "device_gb": _r(f["device_used_bytes"] / 1e9, 3)}
         out["adj384_fp32"] = {"cost_fwd_steps": _r(a["cost_in_forward_steps"], 3),
                               "s_per_step": _r(a["s_per_step"], 3),
                               "peak_gb": _r(a["peak_device_bytes"] / 1e9, 3)}
@@ -675,13 +677,14 @@ def precision_study(L, n: int, steps: int, peak: float):
            "error": f"L2 relative error of u and rho over fluid cells vs the FP64 AA run "
                     f"after {steps} steps", "fp64_aa": r64, "fp64_aa_dense": r64d}
     for name, prec in (("fp32", L.F32), ("fp16", L.F16)):
-        b, r = timed_forward(L, flags, "aa", prec, steps, 0, peak)
-        d = b.compare(ref)
-        r["l2_rel_err_u"] = float(np.sqrt(d[0] / d[1])) if d[1] > 0 else None
-        r["l2_rel_err_rho"] = float(np.sqrt(d[2] / d[3])) if d[3] > 0 else None
-        r["speedup_vs_fp64_aa"] = r["mlups"] / r64["mlups"]
-        res[f"{name}_aa"] = r
-        b.close()
+        for cp in (False, True):
+            b, r = timed_forward(L, flags, "aa", prec, steps, 0, peak, compact=cp)
+            d = b.compare(ref)
+            r["l2_rel_err_u"] = float(np.sqrt(d[0] / d[1])) if d[1] > 0 else None
+            r["l2_rel_err_rho"] = float(np.sqrt(d[2] / d[3])) if d[3] > 0 else None
+            r["speedup_vs_fp64_aa"] = r["mlups"] / r64["mlups"]
+            res[f"{name}_aa" + ("_compact" if cp else "")] = r
+            b.close()
     _, bad = ref.mass_momentum(check=False)
     res["fp64_nonfinite_cells"] = bad
     ref.close()
@@ -720,17 +723,22 @@ def largest_study(L, n: int, steps: int, peak: float, na: int = 384, adj_steps: 
     against the 180 GB HBM."""
     flags, frac, nsph = L.porous_channel((n, n, n), 0.3, 6.0, 12.0, seed=42)
     free0, total = L.device_memory()
-    s, fwd = timed_forward(L, flags, "aa", L.F16, steps, 3, peak)
-    free1, _ = L.device_memory()
-    _, bad = s.mass_momentum(check=False)
-    fwd.update({"workload": f"FP16 porous channel {n}^3 (30% solid, r 6-12), AA, {steps} steps",
-                "nonfinite_cells": bad, "device_used_bytes": total - free1,
-                "device_total_bytes": total, "solid_fraction_achieved": frac, "spheres": nsph})
-    s.close()
+    out = {}
+    for cp in (False, True):
+        s, fwd = timed_forward(L, flags, "aa", L.F16, steps, 3, peak, compact=cp)
+        free1, _ = L.device_memory()
+        _, bad = s.mass_momentum(check=False)
+        fwd.update({"workload": f"FP16 porous channel {n}^3 (30% solid, r 6-12), AA, {steps} "
+                                "steps", "nonfinite_cells": bad,
+                    "device_used_bytes": total - free1, "device_total_bytes": total,
+                    "solid_fraction_achieved": frac, "spheres": nsph})
+        s.close()
+        out["forward_fp16_aa" + ("_compact" if cp else "")] = fwd
     del flags
     a = adjoint_study(L, na, adj_steps, 0, 0, precisions=("fp32",))
     a["fp32"]["device_total_bytes"] = total
-    return {"forward_fp16_aa": fwd, "adjoint": a}
+    out["adjoint"] = a
+    return out
 
 
 def run_largest(args):

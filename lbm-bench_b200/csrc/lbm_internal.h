@@ -28,15 +28,15 @@ cudaError_t launch_step_x2_f32(int kind, bool force, bool brink, const StepArgs2
 cudaError_t launch_step_x2_f16(int kind, bool force, bool brink, const StepArgs2<StoreF16> &a,
     cudaStream_t st);
 
-// Compact (fluid-only) layout steps, one cell per thread (lbm_step_cp.cuh):
-// FP64 in lbm_step_f64.cu (no contraction), FP32/FP16 storage in
-// lbm_step_lp.cu.
+// Compact (fluid-only) layout steps: FP64 one cell per thread
+// (lbm_step_cp.cuh, in lbm_step_f64.cu without contraction), FP32/FP16
+// storage with the pair arithmetic (lbm_step_cp2.cuh, in lbm_step_lp.cu).
 cudaError_t launch_step_cp_f64(int kind, bool force, const StepArgs<StoreF64> &a, dim3 grid,
     dim3 block, cudaStream_t st);
-cudaError_t launch_step_cp_f32(int kind, bool force, const StepArgs<StoreF32> &a, dim3 grid,
-    dim3 block, cudaStream_t st);
-cudaError_t launch_step_cp_f16(int kind, bool force, const StepArgs<StoreF16> &a, dim3 grid,
-    dim3 block, cudaStream_t st);
+cudaError_t launch_step_cp2_f32(int kind, bool force, const StepArgs2<StoreF32> &a,
+    cudaStream_t st);
+cudaError_t launch_step_cp2_f16(int kind, bool force, const StepArgs2<StoreF16> &a,
+    cudaStream_t st);
 
 // Zou-He pressure boundary on the state after a step (lbm_step_f64.cu):
 // marks is [2][ny][nz] (caller's box; 0 = inlet plane x = 0, 1 = outlet

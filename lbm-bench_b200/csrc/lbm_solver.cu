@@ -176,6 +176,9 @@ static Consts2 make_consts2(const lbm_solver *s)
   c.w1NHq = (float)(w1 * 4.5 / S);
   c.w2NHq = (float)(w2 * 4.5 / S);
   c.c15q  = (float)(1.5 / S);
+  // ((S 3 w_d) c_dx) F rounded once: force[inv d] is -force[d] bit for bit,
+  // and force[d] = force[inv d] for c_dx = 0 (the compact local kernel
+  // relies on both)
   for (int d = 0; d < Q; ++d)
     c.force[d] = (float)(S * 3.0 * weight(d) * (double)cx(d) * s->xforce);
   c.alpha = (float)s->alpha;
@@ -1287,32 +1290,34 @@ static int launch_kernel(lbm_solver *s, int x0, int planes, cudaStream_t st, int
       a.c0 = (*s->cplane0)[x0];
       a.cn = (*s->cplane0)[x0 + planes] - a.c0;
       e = launch_step_cp_f64(kind, force, a, grid, block, st);
-    } else if (s->precision == LBM_F32) {
-      StepArgs<StoreF32> a;
-      a.g = s->g;
-      a.src = (const float *)src;
-      a.dst = (float *)dst;
-      a.mask = s->mask;
-      a.porosity = nullptr;
-      a.u_save = nullptr;
-      a.c = make_consts<float>(s);
-      a.x0 = x0;
-      a.c0 = (*s->cplane0)[x0];
-      a.cn = (*s->cplane0)[x0 + planes] - a.c0;
-      e = launch_step_cp_f32(kind, force, a, grid, block, st);
     } else {
-      StepArgs<StoreF16> a;
-      a.g = s->g;
-      a.src = (const __half *)src;
-      a.dst = (__half *)dst;
-      a.mask = s->mask;
-      a.porosity = nullptr;
-      a.u_save = nullptr;
-      a.c = make_consts<float>(s);
-      a.x0 = x0;
-      a.c0 = (*s->cplane0)[x0];
-      a.cn = (*s->cplane0)[x0 + planes] - a.c0;
-      e = launch_step_cp_f16(kind, force, a, grid, block, st);
+      // FP32 / FP16 storage: pair arithmetic, bit-identical to the dense layout
+      StepArgs2<StoreF32> a32;
+      StepArgs2<StoreF16> a16;
+      auto fill = [&](auto &a) {
+        a.g = s->g;
+        a.mask = s->mask;
+        a.porosity = nullptr;
+        a.u_save = nullptr;
+        a.c = make_consts2(s);
+        a.no_shuffle = s->no_shuffle;
+        a.no_quad = s->no_quad;
+        a.x0 = x0;
+        a.planes = planes;
+        a.c0 = (*s->cplane0)[x0];
+        a.cn = (*s->cplane0)[x0 + planes] - a.c0;
+      };
+      if (s->precision == LBM_F32) {
+        fill(a32);
+        a32.src = (const float *)src;
+        a32.dst = (float *)dst;
+        e = launch_step_cp2_f32(kind, force, a32, st);
+      } else {
+        fill(a16);
+        a16.src = (const __half *)src;
+        a16.dst = (__half *)dst;
+        e = launch_step_cp2_f16(kind, force, a16, st);
+      }
     }
   } else if (s->precision == LBM_F64) {
     StepArgs<StoreF64> a;

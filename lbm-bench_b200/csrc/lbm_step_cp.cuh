@@ -135,14 +135,31 @@ template <bool ZPER> struct RowTab {
   }
 };
 
-// OFF: type of element offsets within the state (uint32_t when all 19
-// planes fit below 2^32 elements, which keeps address arithmetic 32-bit).
-template <class ST, int KIND, bool FORCE, bool ZPER, typename OFF>
-__global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND>::value))
-    step_kernel_cp(StepArgs<ST> a)
-{
+// Arithmetic of the compact kernels. CpMathDirect: values as stored and
+// collide() - the FP64 reference arithmetic (bit-identical to LBM-Bench).
+// CpMathUnits (lbm_step_cp2.cuh): FP32/FP16 storage units and the pair
+// kernels' arithmetic, one cell at a time.
+template <class ST> struct CpMathDirect {
+  using Args = StepArgs<ST>;
   using S = typename ST::S;
   using V = typename ST::V;
+  __device__ static V ld(const Args &a, S s) { return ST::decode(s, a.c.inv_scale); }
+  __device__ static S st(const Args &a, V v) { return ST::encode(v, a.c.scale); }
+  __device__ static void coll(const Args &a, const V (&f)[Q], V (&o)[Q])
+  {
+    collide<V, false>(f, o, a.c, V(0));
+  }
+  __device__ static V plus(V x, V y) { return x + y; }
+};
+
+// OFF: type of element offsets within the state (uint32_t when all 19
+// planes fit below 2^32 elements, which keeps address arithmetic 32-bit).
+template <class M, int KIND, bool FORCE, bool ZPER, typename OFF>
+__global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND>::value))
+    step_kernel_cp(typename M::Args a)
+{
+  using S = typename M::S;
+  using V = typename M::V;
   constexpr bool kNC = (KIND == kPullStep || KIND == kPushStep);
   const Grid &g = a.g;
   const int z = blockIdx.x * blockDim.x + threadIdx.x;
@@ -178,13 +195,13 @@ __global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND>::value))
     // local loads: issued without waiting for the mask
 #pragma unroll
     for (int d = 0; d < Q; ++d)
-      f[d] = ST::decode(ldg<kNC>(src + el(d, cell)), a.c.inv_scale);
+      f[d] = M::ld(a, ldg<kNC>(src + el(d, cell)));
   } else if (!__any_sync(__activemask(), (mask & 0x7FFFFu) != 0u)) {
     // no lane of the warp has a wall link: no redirects
 #pragma unroll
     for (int d = 0; d < Q; ++d) {
       const OFF o = (KIND == kPullStep) ? el(d, t.at(g, inv(d))) : el(inv(d), t.at(g, inv(d)));
-      f[d] = ST::decode(ldg<kNC>(src + o), a.c.inv_scale);
+      f[d] = M::ld(a, ldg<kNC>(src + o));
     }
   } else {
 #pragma unroll
@@ -195,17 +212,17 @@ __global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND>::value))
         o = back ? el(inv(d), cell) : el(d, t.at(g, inv(d)));
       else
         o = back ? el(d, cell) : el(inv(d), t.at(g, inv(d)));
-      f[d] = ST::decode(ldg<kNC>(src + o), a.c.inv_scale);
+      f[d] = M::ld(a, ldg<kNC>(src + o));
     }
   }
 
   V o[Q];
-  collide<V, false>(f, o, a.c, V(0));
+  M::coll(a, f, o);
 
 #pragma unroll
   for (int d = 0; d < Q; ++d) {
     const bool bb = (mask >> d) & 1u;
-    const V v = FORCE ? o[d] + (bb ? a.c.force[inv(d)] : a.c.force[d]) : o[d];
+    const V v = FORCE ? M::plus(o[d], bb ? a.c.force[inv(d)] : a.c.force[d]) : o[d];
     OFF off;
     if (KIND == kPullStep)
       off = el(d, cell);
@@ -213,7 +230,7 @@ __global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND>::value))
       off = el(inv(d), cell);
     else
       off = bb ? el(inv(d), cell) : el(d, t.at(g, d));
-    dst[off] = ST::encode(v, a.c.scale);
+    dst[off] = M::st(a, v);
   }
 }
 

@@ -181,7 +181,7 @@ template <class ST, int KIND>
 static cudaError_t go_cp(bool force, const StepArgs<ST> &a, dim3 grid, dim3 block,
     cudaStream_t st)
 {
-  if (KIND == kAAEvenStep) {
+  if constexpr (KIND == kAAEvenStep) {
     if (a.cn == 0)
       return cudaSuccess;
     const unsigned nb = (a.cn + kStepThreads - 1) / kStepThreads;
@@ -190,25 +190,26 @@ static cudaError_t go_cp(bool force, const StepArgs<ST> &a, dim3 grid, dim3 bloc
     else
       step_kernel_cp_local<ST, false><<<nb, kStepThreads, 0, st>>>(a);
     return cudaGetLastError();
-  }
+  } else {
   const bool zper = (a.g.per & 4) != 0;
   const bool off32 = (unsigned long long)Q * (unsigned long long)a.g.plane < (1ull << 32);
   if (off32) {
     if (force)
-      zper ? step_kernel_cp<ST, KIND, true, true, uint32_t><<<grid, block, 0, st>>>(a)
-           : step_kernel_cp<ST, KIND, true, false, uint32_t><<<grid, block, 0, st>>>(a);
+      zper ? step_kernel_cp<CpMathDirect<ST>, KIND, true, true, uint32_t><<<grid, block, 0, st>>>(a)
+           : step_kernel_cp<CpMathDirect<ST>, KIND, true, false, uint32_t><<<grid, block, 0, st>>>(a);
     else
-      zper ? step_kernel_cp<ST, KIND, false, true, uint32_t><<<grid, block, 0, st>>>(a)
-           : step_kernel_cp<ST, KIND, false, false, uint32_t><<<grid, block, 0, st>>>(a);
+      zper ? step_kernel_cp<CpMathDirect<ST>, KIND, false, true, uint32_t><<<grid, block, 0, st>>>(a)
+           : step_kernel_cp<CpMathDirect<ST>, KIND, false, false, uint32_t><<<grid, block, 0, st>>>(a);
   } else {
     if (force)
-      zper ? step_kernel_cp<ST, KIND, true, true, uint64_t><<<grid, block, 0, st>>>(a)
-           : step_kernel_cp<ST, KIND, true, false, uint64_t><<<grid, block, 0, st>>>(a);
+      zper ? step_kernel_cp<CpMathDirect<ST>, KIND, true, true, uint64_t><<<grid, block, 0, st>>>(a)
+           : step_kernel_cp<CpMathDirect<ST>, KIND, true, false, uint64_t><<<grid, block, 0, st>>>(a);
     else
-      zper ? step_kernel_cp<ST, KIND, false, true, uint64_t><<<grid, block, 0, st>>>(a)
-           : step_kernel_cp<ST, KIND, false, false, uint64_t><<<grid, block, 0, st>>>(a);
+      zper ? step_kernel_cp<CpMathDirect<ST>, KIND, false, true, uint64_t><<<grid, block, 0, st>>>(a)
+           : step_kernel_cp<CpMathDirect<ST>, KIND, false, false, uint64_t><<<grid, block, 0, st>>>(a);
   }
   return cudaGetLastError();
+  }
 }
 
 template <class ST>

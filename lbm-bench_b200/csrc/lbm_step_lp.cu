@@ -7,6 +7,7 @@
 #include "lbm_step_x2.cuh"
 #include "lbm_step_x2s.cuh"
 #include "lbm_step_x4s.cuh"
+#include "lbm_step_cp2.cuh"
 
 namespace lbm {
 
@@ -63,7 +64,7 @@ static cudaError_t launch(int kind, bool force, bool brink, const StepArgs2<ST> 
     cudaStream_t st)
 {
   dim3 grid, block;
-  pair_launch_shape(a.g, grid, block);
+  cell_launch_shape(a.g, grid, block);
   grid.z = a.planes;
   switch (kind) {
   case kPullStep: return pick<ST, kPullStep>(force, brink, a, grid, block, st);
@@ -86,63 +87,65 @@ cudaError_t launch_step_x2_f16(int kind, bool force, bool brink, const StepArgs2
   return launch(kind, force, brink, a, st);
 }
 
-template <class ST, int KIND>
-static cudaError_t go_cp(bool force, const StepArgs<ST> &a, dim3 grid, dim3 block,
-    cudaStream_t st)
+template <class ST, int KIND, bool FORCE>
+static cudaError_t go_cp2(const StepArgs2<ST> &a, cudaStream_t st)
 {
-  if (KIND == kAAEvenStep) {
+  if constexpr (KIND == kAAEvenStep) {
+    constexpr uint32_t N = LocalCells<ST>::value;
     if (a.cn == 0)
       return cudaSuccess;
-    const unsigned nb = (a.cn + kStepThreads - 1) / kStepThreads;
-    if (force)
-      step_kernel_cp_local<ST, true><<<nb, kStepThreads, 0, st>>>(a);
-    else
-      step_kernel_cp_local<ST, false><<<nb, kStepThreads, 0, st>>>(a);
+    const uint32_t end = a.c0 + a.cn;
+    const uint32_t lo = (a.c0 + N - 1) / N * N, hi = end / N * N;
+    if (hi > lo) {
+      const uint32_t groups = (hi - lo) / N;
+      step_kernel_cp2_local<ST, FORCE><<<(groups + kStepThreads - 1) / kStepThreads,
+          kStepThreads, 0, st>>>(a);
+    }
+    if (a.c0 % N != 0 || end % N != 0)
+      step_kernel_cp2_local_ends<ST, FORCE><<<1, 32, 0, st>>>(a);
     return cudaGetLastError();
-  }
+  } else {
+  dim3 grid, block;
+  cell_launch_shape(a.g, grid, block);
+  grid.z = a.planes;
   const bool zper = (a.g.per & 4) != 0;
   const bool off32 = (unsigned long long)Q * (unsigned long long)a.g.plane < (1ull << 32);
-  if (off32) {
-    if (force)
-      zper ? step_kernel_cp<ST, KIND, true, true, uint32_t><<<grid, block, 0, st>>>(a)
-           : step_kernel_cp<ST, KIND, true, false, uint32_t><<<grid, block, 0, st>>>(a);
-    else
-      zper ? step_kernel_cp<ST, KIND, false, true, uint32_t><<<grid, block, 0, st>>>(a)
-           : step_kernel_cp<ST, KIND, false, false, uint32_t><<<grid, block, 0, st>>>(a);
-  } else {
-    if (force)
-      zper ? step_kernel_cp<ST, KIND, true, true, uint64_t><<<grid, block, 0, st>>>(a)
-           : step_kernel_cp<ST, KIND, true, false, uint64_t><<<grid, block, 0, st>>>(a);
-    else
-      zper ? step_kernel_cp<ST, KIND, false, true, uint64_t><<<grid, block, 0, st>>>(a)
-           : step_kernel_cp<ST, KIND, false, false, uint64_t><<<grid, block, 0, st>>>(a);
-  }
+  if (off32)
+    zper ? step_kernel_cp<CpMathUnits<ST>, KIND, FORCE, true, uint32_t><<<grid, block, 0, st>>>(a)
+         : step_kernel_cp<CpMathUnits<ST>, KIND, FORCE, false, uint32_t><<<grid, block, 0, st>>>(a);
+  else
+    zper ? step_kernel_cp<CpMathUnits<ST>, KIND, FORCE, true, uint64_t><<<grid, block, 0, st>>>(a)
+         : step_kernel_cp<CpMathUnits<ST>, KIND, FORCE, false, uint64_t><<<grid, block, 0, st>>>(a);
   return cudaGetLastError();
+  }
 }
 
 template <class ST>
-static cudaError_t launch_cp(int kind, bool force, const StepArgs<ST> &a, dim3 grid, dim3 block,
-    cudaStream_t st)
+static cudaError_t launch_cp2(int kind, bool force, const StepArgs2<ST> &a, cudaStream_t st)
 {
   switch (kind) {
-  case kPullStep: return go_cp<ST, kPullStep>(force, a, grid, block, st);
-  case kPushStep: return go_cp<ST, kPushStep>(force, a, grid, block, st);
-  case kAAEvenStep: return go_cp<ST, kAAEvenStep>(force, a, grid, block, st);
-  case kAAOddStep: return go_cp<ST, kAAOddStep>(force, a, grid, block, st);
+  case kPullStep: return force ? go_cp2<ST, kPullStep, true>(a, st)
+                               : go_cp2<ST, kPullStep, false>(a, st);
+  case kPushStep: return force ? go_cp2<ST, kPushStep, true>(a, st)
+                               : go_cp2<ST, kPushStep, false>(a, st);
+  case kAAEvenStep: return force ? go_cp2<ST, kAAEvenStep, true>(a, st)
+                                 : go_cp2<ST, kAAEvenStep, false>(a, st);
+  case kAAOddStep: return force ? go_cp2<ST, kAAOddStep, true>(a, st)
+                                : go_cp2<ST, kAAOddStep, false>(a, st);
   }
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_step_cp_f32(int kind, bool force, const StepArgs<StoreF32> &a, dim3 grid,
-    dim3 block, cudaStream_t st)
+cudaError_t launch_step_cp2_f32(int kind, bool force, const StepArgs2<StoreF32> &a,
+    cudaStream_t st)
 {
-  return launch_cp<StoreF32>(kind, force, a, grid, block, st);
+  return launch_cp2<StoreF32>(kind, force, a, st);
 }
 
-cudaError_t launch_step_cp_f16(int kind, bool force, const StepArgs<StoreF16> &a, dim3 grid,
-    dim3 block, cudaStream_t st)
+cudaError_t launch_step_cp2_f16(int kind, bool force, const StepArgs2<StoreF16> &a,
+    cudaStream_t st)
 {
-  return launch_cp<StoreF16>(kind, force, a, grid, block, st);
+  return launch_cp2<StoreF16>(kind, force, a, st);
 }
 
 } // namespace lbm

@@ -113,6 +113,50 @@ __device__ __forceinline__ void collide2(const float2 (&f)[Q], float2 (&o)[Q], c
   pair(dTN, dBS, add2(uy, uz), c.w2NHq, c.w2X3, w2D);
 }
 
+// collide2 for one cell: the same IEEE operations in the same order on
+// scalars, so a cell collided alone gets exactly the value it gets as one
+// half of a pair.
+__device__ __forceinline__ void collide1(const float (&f)[Q], float (&o)[Q], const Consts2 &c)
+{
+  auto add = [](float a, float b) { return __fadd_rn(a, b); };
+  auto sub = [](float a, float b) { return __fadd_rn(a, -b); };
+  auto mul = [](float a, float b) { return __fmul_rn(a, b); };
+  auto fma = [](float a, float b, float d) { return __fmaf_rn(a, b, d); };
+  const float ux = sub(add(add(add(add(f[dE], f[dNE]), f[dSE]), f[dTE]), f[dBE]),
+      add(add(add(add(f[dW], f[dNW]), f[dSW]), f[dTW]), f[dBW]));
+  const float uy = sub(add(add(add(add(f[dN], f[dNE]), f[dNW]), f[dTN]), f[dBN]),
+      add(add(add(add(f[dS], f[dSE]), f[dSW]), f[dTS]), f[dBS]));
+  const float uz = sub(add(add(add(add(f[dT], f[dTE]), f[dTW]), f[dTN]), f[dTS]),
+      add(add(add(add(f[dB], f[dBE]), f[dBW]), f[dBN]), f[dBS]));
+  float dens = f[dC];
+#pragma unroll
+  for (int d = 0; d < Q - 1; ++d)
+    dens = add(dens, f[d]);
+  const float usq = fma(uz, uz, fma(uy, uy, mul(ux, ux)));
+  const float D = fma(-c.c15q, usq, dens);
+  const float oE = c.oE, oO = c.oO, h = 0.5f;
+  o[dC] = fma(oE, fma(c.w0, D, -f[dC]), f[dC]);
+  const float w1D = mul(c.w1, D), w2D = mul(c.w2, D);
+  auto pair = [&](int a, int b, float ui, float wnhq, float wx3, float wD) {
+    const float sum = add(f[a], f[b]), dif = sub(f[a], f[b]);
+    const float q = fma(wnhq, mul(ui, ui), wD);
+    const float evenPart = mul(oE, fma(h, sum, -q));
+    const float uw = mul(ui, wx3);
+    const float oddPart = mul(oO, fma(h, dif, -uw));
+    o[a] = sub(sub(f[a], evenPart), oddPart);
+    o[b] = add(sub(f[b], evenPart), oddPart);
+  };
+  pair(dN, dS, uy, c.w1NHq, c.w1X3, w1D);
+  pair(dE, dW, ux, c.w1NHq, c.w1X3, w1D);
+  pair(dT, dB, uz, c.w1NHq, c.w1X3, w1D);
+  pair(dNW, dSE, sub(uy, ux), c.w2NHq, c.w2X3, w2D);
+  pair(dNE, dSW, add(ux, uy), c.w2NHq, c.w2X3, w2D);
+  pair(dTW, dBE, sub(uz, ux), c.w2NHq, c.w2X3, w2D);
+  pair(dTE, dBW, add(ux, uz), c.w2NHq, c.w2X3, w2D);
+  pair(dTS, dBN, sub(uz, uy), c.w2NHq, c.w2X3, w2D);
+  pair(dTN, dBS, add(uy, uz), c.w2NHq, c.w2X3, w2D);
+}
+
 template <class ST> struct StepArgs2 {
   using S = typename ST::S;
   Grid g;
@@ -126,6 +170,7 @@ template <class ST> struct StepArgs2 {
   int no_quad;    // host-side switch: AA in FP16 storage on the two-cell kernels
   int x0 = 0;     // first storage x plane of the launch (grid.z planes from there)
   int planes = 0; // x planes of the launch
+  uint32_t c0 = 0, cn = 0; // compact layout, local steps: storage indices [c0, c0 + cn)
 };
 
 // Minimum resident CTAs per SM of the pair kernels, per storage type and

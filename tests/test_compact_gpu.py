@@ -106,11 +106,13 @@ def test_compact_fluid_on_non_periodic_faces(oracle):
 
 @pytest.mark.parametrize("precision", [L.F32, L.F16])
 @pytest.mark.parametrize("pattern", PATTERNS)
-def test_compact_reduced_precision_matches_dense(pattern, precision):
-    """FP32/FP16 storage: the compact layout's one-cell kernel and the dense
-    layout's pair kernels round differently in places, so they agree to
-    within the storage precision, and both stay close to FP64."""
-    flags, _, _ = L.porous_channel((40, 36, 64), 0.2, 3.0, 5.0, seed=8)
+@pytest.mark.parametrize("dims", [(40, 36, 64), (23, 17, 45)])
+def test_compact_reduced_precision_bit_identical_to_dense(pattern, precision, dims):
+    """FP32/FP16 storage: the compact layout's pair kernels apply to every
+    cell the operations of the dense layout's pair kernels, so the states are
+    bit-identical; both stay close to FP64. nz = 45 is odd (a pair with a
+    padding cell at the row end) and not a multiple of 32."""
+    flags, _, _ = L.porous_channel(dims, 0.2, 3.0, 5.0, seed=8)
     f0 = L.perturbed_equilibrium(flags, seed=3, amplitude=1e-4)
     steps = 24
     c = run(flags, (1, 0, 0), f0, steps, 1.25, 3 / 16, 1e-6, True, pattern, precision)
@@ -118,9 +120,56 @@ def test_compact_reduced_precision_matches_dense(pattern, precision):
             compact=False)
     r = run(flags, (1, 0, 0), f0, steps, 1.25, 3 / 16, 1e-6, True, pattern, L.F64)
     m = O.fluid_mask(flags)
+    assert np.array_equal(c[:, m], d[:, m])
     tol = 1e-6 if precision == L.F32 else 2e-4
-    assert np.abs(c[:, m] - d[:, m]).max() < tol
     assert np.abs(c[:, m] - r[:, m]).max() < tol
+
+
+@pytest.mark.parametrize("precision", [L.F64, L.F32, L.F16])
+@pytest.mark.parametrize("per", [(1, 0, 0), (1, 1, 1)])
+def test_compact_reduced_precision_random_geometries(oracle, precision, per):
+    """Random obstacles with periodic y and z too (the pair kernels'
+    wrapped-neighbour path): compact equals dense bit for bit."""
+    rng = np.random.default_rng(41 + sum(per))
+    nx, ny, nz = 9, 11, 37
+    flags = (rng.uniform(size=(nz, ny, nx)) > 0.3).astype(np.int32)
+    if not per[1]:
+        flags[:, [0, -1], :] = 0
+    if not per[2]:
+        flags[[0, -1], :, :] = 0
+    f0 = O.perturbed_state(flags, 5, amp=2e-3)
+    m = O.fluid_mask(flags)
+    for pattern in PATTERNS:
+        c = run(flags, per, f0, 7, 1.3, 3 / 16, 2e-6, True, pattern, precision)
+        d = run(flags, per, f0, 7, 1.3, 3 / 16, 2e-6, True, pattern, precision, compact=False)
+        assert np.array_equal(c[:, m], d[:, m]), pattern
+
+
+@pytest.mark.parametrize("precision", [L.F64, L.F32, L.F16])
+def test_compact_split_steps_equal_whole_steps(precision):
+    """Steps launched as several x-plane ranges (lbm_step_begin / _planes /
+    _end) cover storage ranges that start and end anywhere: the local AA
+    even kernel's partial groups at both ends must give the whole step's
+    state."""
+    flags, _, _ = L.porous_channel((17, 13, 30), 0.25, 2.0, 4.0, seed=6)
+    f0 = L.perturbed_equilibrium(flags, seed=2, amplitude=1e-3)
+    cuts = [0, 3, 4, 9, 10, 16, 17]
+    states = []
+    for split in (False, True):
+        with L.Solver(flags, (1, 0, 0), "aa", precision, compact=True) as s:
+            s.set_params(1.2, 3 / 16, 1e-6, True)
+            s.set_state(f0)
+            for _ in range(6):
+                if split:
+                    s.step_begin()
+                    for a, b in zip(cuts[:-1], cuts[1:]):
+                        s.step_planes(a, b, side=(a % 2 == 1))
+                    s.step_end()
+                else:
+                    s.run(1)
+            states.append(s.get_state())
+    m = O.fluid_mask(flags)
+    assert np.array_equal(states[0][:, m], states[1][:, m])
 
 
 def test_compact_reductions_and_transfers_equal_dense():
