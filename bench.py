@@ -777,7 +777,7 @@ def run_slabs(args, dist: Dist):
     f0 = L.perturbed_equilibrium(own, seed=7, amplitude=1e-4)
     peak, peak_kind = measured_hbm_peak()
 
-    s = L.Solver.slab(sflags, (0, 0), "aa", L.F64)
+    s = L.Solver.slab(sflags, (0, 0), "aa", L.F64, compact=args.layout == "compact")
     s.set_params(1.25, 3 / 16, 1e-6, True)
     s.set_state(f0)
     runner = lbm_slab.SlabRunner(s, lbm_slab.Ring(), overlap=True)
@@ -835,6 +835,7 @@ def run_slabs(args, dist: Dist):
                                           "per GPU), 20% solid spheres r 4-8, seed 42",
                        dims=[n * world, n, n], solid_fraction_achieved=frac, spheres=nsph,
                        fluid_cells=int(total_fluid), parallelism=f"x-slabs x{world}",
+                       layout=args.layout,
                        halo="5 populations x 256 x 256 per face, before and after each odd "
                             "AA step, NCCL send/recv between ring neighbours, overlapped with "
                             "the interior planes' update on a second stream"),

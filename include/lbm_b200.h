@@ -72,6 +72,12 @@ int lbm_create(lbm_solver **out, int nx, int ny, int nz, const int *flags, int p
 int lbm_create_slab(lbm_solver **out, int nx, int ny, int nz, const int *flags, int periodic_y,
     int periodic_z, int pattern, int precision);
 
+/* The same slab in the compact layout (lbm_create_compact): the fluid cells
+ * of its own planes and of both ghost planes are stored; the halo calls
+ * exchange the same messages as for a dense slab (a solid cell sends 0). */
+int lbm_create_slab_compact(lbm_solver **out, int nx, int ny, int nz, const int *flags,
+    int periodic_y, int periodic_z, int pattern, int precision);
+
 /* The same solver in the compact (fluid-only) layout: populations and link
  * masks are stored for fluid cells only, packed row by row in z order, so no
  * obstacle cell shares a memory sector with a fluid one and every byte moved
@@ -79,7 +85,7 @@ int lbm_create_slab(lbm_solver **out, int nx, int ny, int nz, const int *flags, 
  * (src/kernel_pull_soa.c:94-96) and has no such layout. Results are
  * identical to lbm_create's (FP64: bit for bit, like the reference); every
  * call below works on it except lbm_set_porosity / lbm_adjoint_gradient
- * (no Brinkman term) and the slab calls. */
+ * (no Brinkman term). Slabs: lbm_create_slab_compact. */
 int lbm_create_compact(lbm_solver **out, int nx, int ny, int nz, const int *flags,
     int periodic_x, int periodic_y, int periodic_z, int pattern, int precision);
 

@@ -658,7 +658,7 @@ static int create_impl(lbm_solver **out, int nx, int ny, int nz, const int *flag
   // compact layout: one fluid bit per cell and the storage index of the
   // first fluid cell of every 32-cell word, rows in (x, y) order
   std::vector<uint32_t> hbits, hbase;
-  s->compact = compact && !slab;
+  s->compact = compact;
   if (s->compact) {
     const int W = (s->g.nz + 31) / 32;
     const size_t rows = (size_t)s->g.nx * s->g.ny;
@@ -848,6 +848,13 @@ extern "C" int lbm_create_compact(lbm_solver **out, int nx, int ny, int nz, cons
 }
 
 extern "C" int lbm_is_compact(const lbm_solver *s) { return s ? s->compact : -1; }
+
+extern "C" int lbm_create_slab_compact(lbm_solver **out, int nx, int ny, int nz,
+    const int *flags, int periodic_y, int periodic_z, int pattern, int precision)
+{
+  return create_impl(out, nx, ny, nz, flags, 0, periodic_y, periodic_z, pattern, precision, 1,
+      1);
+}
 
 extern "C" int lbm_create_slab(lbm_solver **out, int nx, int ny, int nz, const int *flags,
     int periodic_y, int periodic_z, int pattern, int precision)
@@ -1402,7 +1409,11 @@ static int launch_one(lbm_solver *s, int *kind_out)
 {
   if (s->split)
     return fail(LBM_ERR_STATE, "a split step is open (lbm_step_begin without lbm_step_end)");
-  int rc = launch_kernel(s, 0, s->g.nx, s->stream, kind_out);
+  // the compact layout stores the fluid cells of a slab's ghost planes too
+  // (they are read and written by the boundary planes' steps), and its
+  // kernels select cells by their fluid bit: launch the own planes only
+  const int gx = (s->compact && s->slab) ? 1 : 0;
+  int rc = launch_kernel(s, gx, s->g.nx - 2 * gx, s->stream, kind_out);
   return rc ? rc : finish_step(s);
 }
 
@@ -1793,9 +1804,23 @@ __global__ void halo_copy_kernel(Grid g, UserBox u, int xplane, int sgn, T *stat
   if (z >= u.nz || y >= u.ny)
     return;
   const int d = halo_dir(sgn, k);
-  const uint32_t cell = cell_index(g, xplane, y + u.oy, z + u.oz);
-  const size_t si = (size_t)d * g.plane + cell;
   const size_t bi = ((size_t)k * u.ny + y) * u.nz + z;
+  uint32_t cell;
+  if (g.bits) {
+    // compact layout: only stored (fluid) cells take part; a solid cell
+    // sends 0 and receives nothing
+    const uint32_t wk = ((uint32_t)xplane * (uint32_t)g.ny + (uint32_t)(y + u.oy)) *
+        (uint32_t)g.W + (uint32_t)((z + u.oz) >> 5);
+    if (!((g.bits[wk] >> ((z + u.oz) & 31)) & 1u)) {
+      if (to_buf)
+        buf[bi] = T(0);
+      return;
+    }
+    cell = packed_index(g, xplane, y + u.oy, z + u.oz);
+  } else {
+    cell = cell_index(g, xplane, y + u.oy, z + u.oz);
+  }
+  const size_t si = (size_t)d * g.plane + cell;
   if (to_buf) {
     buf[bi] = state[si];
     return;

@@ -51,6 +51,9 @@ _SIGNATURES = [
                                           ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("lbm_is_compact", ctypes.c_int, [_vp]),
+    ("lbm_create_slab_compact", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_int]),
     ("lbm_create_slab", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, ctypes.c_int]),
@@ -176,10 +179,11 @@ class Solver:
         return lib().lbm_is_compact(self._h) == 1
 
     @classmethod
-    def slab(cls, flags, periodic_yz=(0, 0), pattern=AA, precision=F64):
-        """x-slab of a decomposed domain (lbm_create_slab): `flags` has the
-        slab's planes plus the neighbours' boundary planes at x = 0 and
-        x = -1 (shape (nz, ny, nx + 2))."""
+    def slab(cls, flags, periodic_yz=(0, 0), pattern=AA, precision=F64, compact=False):
+        """x-slab of a decomposed domain (lbm_create_slab, or
+        lbm_create_slab_compact with compact=True): `flags` has the slab's
+        planes plus the neighbours' boundary planes at x = 0 and x = -1
+        (shape (nz, ny, nx + 2))."""
         self = cls.__new__(cls)
         if isinstance(pattern, str):
             pattern = PATTERNS[pattern]
@@ -193,8 +197,9 @@ class Solver:
         self.pattern, self.precision = pattern, precision
         self.periodic = (0,) + tuple(int(p) for p in periodic_yz)
         h = _vp()
-        _check(lib().lbm_create_slab(ctypes.byref(h), nx, ny, nz, _p(flags, _ip),
-                                     *self.periodic[1:], pattern, precision))
+        create = lib().lbm_create_slab_compact if compact else lib().lbm_create_slab
+        _check(create(ctypes.byref(h), nx, ny, nz, _p(flags, _ip), *self.periodic[1:], pattern,
+                      precision))
         self._h = h
         return self
 

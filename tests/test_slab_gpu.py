@@ -1,7 +1,7 @@
-"""x-slab decomposition on a B200: slabs made by lbm_create_slab and
-exchanging halos (lbm_halo_pack / lbm_halo_unpack) reproduce the
-undecomposed x-periodic solver bit for bit, for every propagation pattern
-and storage precision. The slabs of a ring run in one process on one GPU
+"""x-slab decomposition on a B200: slabs made by lbm_create_slab (or
+lbm_create_slab_compact) and exchanging halos (lbm_halo_pack /
+lbm_halo_unpack) reproduce the undecomposed x-periodic solver bit for bit,
+for every propagation pattern, storage precision and layout. The slabs of a ring run in one process on one GPU
 (lbm_slab.LocalRing: pack all, synchronise, unpack all), and one slab runs
 through lbm_slab.SlabRunner as a ring of one."""
 import numpy as np
@@ -26,34 +26,36 @@ def _params(s):
     s.set_params(1.25, 3 / 16, 1e-5, True)
 
 
-def _single(flags, f0, pattern, precision, steps):
-    with L.Solver(flags, (1, 0, 0), pattern, precision) as s:
+def _single(flags, f0, pattern, precision, steps, compact=False):
+    with L.Solver(flags, (1, 0, 0), pattern, precision, compact=compact) as s:
         _params(s)
         s.set_state(f0)
         s.run(steps)
         return s.get_state(), s.mass_momentum()[0]
 
 
-def _slabs(flags, f0, pattern, precision, world):
+def _slabs(flags, f0, pattern, precision, world, compact=False):
     nx = flags.shape[2]
     out = []
     for r in range(world):
         x0, x1 = lbm_slab.split(nx, world, r)
-        s = L.Solver.slab(lbm_slab.slab_flags(flags, x0, x1), (0, 0), pattern, precision)
+        s = L.Solver.slab(lbm_slab.slab_flags(flags, x0, x1), (0, 0), pattern, precision,
+                          compact=compact)
         _params(s)
         s.set_state(np.ascontiguousarray(f0[:, x0:x1]))
         out.append(s)
     return out
 
 
+@pytest.mark.parametrize("compact", [False, True], ids=["dense", "compact"])
 @pytest.mark.parametrize("precision", [L.F64, L.F32, L.F16])
 @pytest.mark.parametrize("pattern", PATTERNS)
 @pytest.mark.parametrize("world", [2, 3])
-def test_local_ring_equals_undecomposed(pattern, precision, world):
+def test_local_ring_equals_undecomposed(pattern, precision, world, compact):
     flags, f0 = _domain((23, 14, 12), 3 + world)
     steps = 9
     ref, tot_ref = _single(flags, f0, pattern, precision, steps)
-    slabs = _slabs(flags, f0, pattern, precision, world)
+    slabs = _slabs(flags, f0, pattern, precision, world, compact)
     ring = lbm_slab.LocalRing(slabs)
     ring.scatter()
     ring.run(steps)
@@ -105,10 +107,11 @@ def test_slab_runner_ring_of_one_is_periodic(pattern):
     assert ex == expect
 
 
+@pytest.mark.parametrize("compact", [False, True], ids=["dense", "compact"])
 @pytest.mark.parametrize("precision", [L.F64, L.F32, L.F16])
 @pytest.mark.parametrize("pattern", PATTERNS)
 @pytest.mark.parametrize("dims", [(18, 12, 10), (9, 6, 128), (2, 8, 64), (1, 9, 7)])
-def test_split_steps_ring_of_one_equal_undecomposed(pattern, precision, dims):
+def test_split_steps_ring_of_one_equal_undecomposed(pattern, precision, dims, compact):
     """SlabRunner(overlap=True): each step split into the interior planes on
     the solver's second stream and the boundary planes plus exchanges on its
     own stream (lbm_step_begin / _planes / _end), bit for bit equal to the
@@ -116,7 +119,7 @@ def test_split_steps_ring_of_one_equal_undecomposed(pattern, precision, dims):
     of 1 and 2 planes have no interior."""
     flags, f0 = _domain(dims, 31)
     ref, _ = _single(flags, f0, pattern, precision, 7)
-    s = _slabs(flags, f0, pattern, precision, 1)[0]
+    s = _slabs(flags, f0, pattern, precision, 1, compact)[0]
     runner = lbm_slab.SlabRunner(s, lbm_slab.Ring(), overlap=True)
     runner.scatter()
     launches0 = s.launch_count
@@ -130,11 +133,12 @@ def test_split_steps_ring_of_one_equal_undecomposed(pattern, precision, dims):
     assert split_launches == 7 * min(dims[0], 3)
 
 
+@pytest.mark.parametrize("compact", [False, True], ids=["dense", "compact"])
 @pytest.mark.parametrize("pattern", PATTERNS)
-def test_split_steps_on_a_ring_of_three(pattern):
+def test_split_steps_on_a_ring_of_three(pattern, compact):
     flags, f0 = _domain((23, 14, 12), 17)
     ref, _ = _single(flags, f0, pattern, L.F64, 9)
-    slabs = _slabs(flags, f0, pattern, L.F64, 3)
+    slabs = _slabs(flags, f0, pattern, L.F64, 3, compact)
     ring = lbm_slab.LocalRing(slabs, overlap=True)
     ring.scatter()
     ring.run(9)
