@@ -455,6 +455,8 @@ def summary(r):
                              "bitwise": q[c]["bit_identical"], "steps": q[c]["steps"]}
                          for c in ("config0", "config1")}
     out["e2e_mlups"] = _r(r["e2e"]["value"])
+    if "transfer_gbs" in r["e2e"]:
+        out["e2e_transfer_gbs"] = _r(r["e2e"]["transfer_gbs"], 3)
     cb = r.get("cpu_baseline")
     if cb and cb.get("value"):
         out["cpu_ref_mlups"] = _r(cb["value"])
@@ -864,14 +866,17 @@ def run_e2e(L, flags, f0, steps, dist: Dist):
         host[:, 1:-1, 1:-1, 1:-1] = f0
         dist.barrier()
         t0 = time.perf_counter()
-        k.run(steps)
+        device_s = float(k.run(steps))  # kd->Duration: the step loop alone (CUDA events)
         t = time.perf_counter() - t0
         n_fluid = int((flags != 0).sum())
         nbytes = host.nbytes
     t = dist.max(t)
+    transfer_s = max(t - device_s, 1e-9)
     return {"value": dist.world * n_fluid * steps / t / 1e6, "unit": "MLUPS",
             "h2d_bytes_per_step": nbytes / steps, "d2h_bytes_per_step": nbytes / steps,
             "h2d_bytes_per_call": nbytes, "d2h_bytes_per_call": nbytes, "seconds": t,
+            "step_loop_seconds": device_s, "transfer_seconds": transfer_s,
+            "transfer_gbs": 2 * nbytes / transfer_s / 1e9,
             "call": "kernelInitCudaAaSoA + kd->Kernel (host arrays in the reference's padded "
                     "layout, page-locked; upload + steps + download inside the timing)"}
 

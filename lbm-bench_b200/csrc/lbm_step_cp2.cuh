@@ -57,19 +57,8 @@ __device__ __forceinline__ void cp2_local_pair(const StepArgs2<ST> &a, const flo
 #pragma unroll
   for (int d = 0; d < Q; ++d) {
     float2 v = out[d];
-    if (FORCE) {
-      // a bounced population carries force[inv d]: for c_x = 0 that equals
-      // force[d] (the same signed zero), otherwise it is -force[d] bit for
-      // bit (the constants are rounded products with the sign of c_x), so
-      // the select is a sign flip and needs no branch
-      if (cx(d) == 0) {
-        v = add2(v, f2(a.c.force[d]));
-      } else {
-        const uint32_t fb = __float_as_uint(a.c.force[d]);
-        v = add2(v, make_float2(__uint_as_float(fb ^ (((m0 >> d) & 1u) << 31)),
-                                __uint_as_float(fb ^ (((m1 >> d) & 1u) << 31))));
-      }
-    }
+    if (FORCE)
+      v = add_force2(v, d, m0, m1, a.c.force);
     typename PT::S *p = a.dst + inv(d) * PL + c;
     if (vec) {
       *reinterpret_cast<P *>(p) = PT::enc(v);

@@ -31,6 +31,22 @@ struct Consts2 {
   float alpha;
 };
 
+// v + the body force a population of direction d carries into each cell of
+// a pair: force[d], or force[inv d] for a population that bounces back at
+// the pair's cell (bit d of m0 / m1). For c_x = 0 both are the same signed
+// zero; otherwise force[inv d] is -force[d] bit for bit (Consts2 rounds one
+// product with the sign of c_x), so the select is a sign flip, with no
+// branch and the same result as selecting the constant.
+__device__ __forceinline__ float2 add_force2(float2 v, int d, uint32_t m0, uint32_t m1,
+    const float (&force)[Q])
+{
+  if (cx(d) == 0)
+    return __fadd2_rn(v, make_float2(force[d], force[d]));
+  const uint32_t fb = __float_as_uint(force[d]);
+  return __fadd2_rn(v, make_float2(__uint_as_float(fb ^ (((m0 >> d) & 1u) << 31)),
+                                   __uint_as_float(fb ^ (((m1 >> d) & 1u) << 31))));
+}
+
 template <class ST> struct PairOf;
 template <> struct PairOf<StoreF32> {
   using S = float;
@@ -284,11 +300,7 @@ __global__ void __launch_bounds__(kStepThreads, (PairOccupancy<ST, KIND, false>:
       // never read, so both cells are written.
       float2 v = out[d];
       if (FORCE) {
-        if (links)
-          v = add2(v, make_float2(bb0 ? a.c.force[inv(d)] : a.c.force[d],
-                                  bb1 ? a.c.force[inv(d)] : a.c.force[d]));
-        else
-          v = add2(v, f2(a.c.force[d]));
+        v = add_force2(v, d, m0, m1, a.c.force);
       }
       const int pl = (KIND == kPullStep) ? d : inv(d);
       *reinterpret_cast<P *>(dst + pl * PL + cell) = PT::enc(v);
@@ -353,7 +365,6 @@ __global__ void __launch_bounds__(kStepThreads, LBM_MINB_QUAD)
     const uint32_t m0 = h ? mq.z : mq.x, m1 = h ? mq.w : mq.y;
     if ((m0 & kSolidBit) && (m1 & kSolidBit))
       continue;
-    const bool links = ((m0 | m1) & 0x7FFFFu) != 0u;
     float2 f[Q];
 #pragma unroll
     for (int d = 0; d < Q; ++d) {
@@ -364,14 +375,9 @@ __global__ void __launch_bounds__(kStepThreads, LBM_MINB_QUAD)
     collide2<false>(f, out, a.c, f2(0.f), nullptr);
 #pragma unroll
     for (int d = 0; d < Q; ++d) {
-      const bool bb0 = (m0 >> d) & 1u, bb1 = (m1 >> d) & 1u;
       float2 v = out[d];
       if (FORCE) {
-        if (links)
-          v = add2(v, make_float2(bb0 ? a.c.force[inv(d)] : a.c.force[d],
-                                  bb1 ? a.c.force[inv(d)] : a.c.force[d]));
-        else
-          v = add2(v, f2(a.c.force[d]));
+        v = add_force2(v, d, m0, m1, a.c.force);
       }
       *reinterpret_cast<P *>(a.dst + inv(d) * PL + cell + 2 * h) = PT::enc(v);
     }

@@ -168,11 +168,7 @@ __global__ void __launch_bounds__(kStepThreads, LBM_MINB_X4S)
         // local store (d, x); a bounced population carries F_inv d
         float2 v = out[d];
         if (FORCE) {
-          if (links)
-            v = add2(v, make_float2(bb0 ? a.c.force[inv(d)] : a.c.force[d],
-                                    bb1 ? a.c.force[inv(d)] : a.c.force[d]));
-          else
-            v = add2(v, f2(a.c.force[d]));
+          v = add_force2(v, d, m0, m1, a.c.force);
         }
         *reinterpret_cast<P *>(dst + d * PL + cell + 2 * h) = PT::enc(v);
         continue;
