@@ -119,6 +119,16 @@ int lbm_set_porosity(lbm_solver *s, const float *porosity, double alpha);
 int lbm_set_state(lbm_solver *s, const double *f);
 int lbm_get_state(lbm_solver *s, double *f);
 
+/* Checkpoint / resume on the host. lbm_save_state writes the state (as
+ * lbm_get_state returns it, FP64) and the step count to a file;
+ * lbm_load_state reads it into a solver of the same box, geometry (fluid
+ * cell count) and pattern and continues from that step, so an AA solver
+ * resumes in the right orientation. A solver of the same precision (and
+ * FP16 scale) continues bit for bit; another precision converts. No
+ * counterpart in the reference (it keeps no state between runs). */
+int lbm_save_state(lbm_solver *s, const char *path);
+int lbm_load_state(lbm_solver *s, const char *path);
+
 /* Orientation of a state held in LBM-Bench's own padded SoA array
  * (indexSoA with a one-cell ghost layer, (nx+2)*(ny+2)*(nz+2) values per
  * direction, src/lbm.h:113-116): where kd->GetNode finds f_d(x)

@@ -1007,6 +1007,103 @@ extern "C" int lbm_get_state(lbm_solver *s, double *f)
 }
 
 // ---------------------------------------------------------------------------
+// Checkpoint / resume of a solver's state on the host
+// ---------------------------------------------------------------------------
+
+// File: this header, then the state as lbm_get_state returns it (FP64,
+// f[d][x][y][z], little-endian). Decoding FP32/FP16 storage to FP64 and
+// encoding it again are exact, so a solver of the same precision (and FP16
+// scale) that loads the file continues bit for bit.
+struct StateFileHeader {
+  char magic[8];        // "LBMB200S"
+  uint32_t version;     // 1
+  int32_t nx, ny, nz;
+  int32_t pattern, precision;
+  int64_t steps_done;   // sets the orientation the state continues from
+  int64_t fluid_cells;  // must match the loading solver's geometry
+  double fp16_scale;
+};
+static const char kStateMagic[8] = { 'L', 'B', 'M', 'B', '2', '0', '0', 'S' };
+
+extern "C" int lbm_save_state(lbm_solver *s, const char *path)
+{
+  if (!s || !path)
+    return fail(LBM_ERR_ARG, "lbm_save_state: NULL argument");
+  std::vector<double> f;
+  try {
+    f.resize((size_t)Q * s->nx * s->ny * s->nz);
+  } catch (...) {
+    return fail(LBM_ERR_ALLOC, "lbm_save_state: host allocation failed");
+  }
+  int rc = lbm_get_state(s, f.data());
+  if (rc)
+    return rc;
+  StateFileHeader h;
+  memset(&h, 0, sizeof(h));
+  memcpy(h.magic, kStateMagic, 8);
+  h.version = 1;
+  h.nx = s->nx;
+  h.ny = s->ny;
+  h.nz = s->nz;
+  h.pattern = s->pattern;
+  h.precision = s->precision;
+  h.steps_done = s->steps_done;
+  h.fluid_cells = s->n_fluid;
+  h.fp16_scale = s->fp16_scale;
+  FILE *fp = fopen(path, "wb");
+  if (!fp)
+    return fail(LBM_ERR_ARG, "lbm_save_state: cannot open %s for writing", path);
+  const bool ok = fwrite(&h, sizeof(h), 1, fp) == 1 && fwrite(f.data(), sizeof(double), f.size(),
+      fp) == f.size();
+  if (fclose(fp) != 0 || !ok)
+    return fail(LBM_ERR_ARG, "lbm_save_state: writing %s failed", path);
+  return LBM_OK;
+}
+
+extern "C" int lbm_load_state(lbm_solver *s, const char *path)
+{
+  if (!s || !path)
+    return fail(LBM_ERR_ARG, "lbm_load_state: NULL argument");
+  if (s->split)
+    return fail(LBM_ERR_STATE, "lbm_load_state: a split step is open");
+  FILE *fp = fopen(path, "rb");
+  if (!fp)
+    return fail(LBM_ERR_ARG, "lbm_load_state: cannot open %s", path);
+  StateFileHeader h;
+  if (fread(&h, sizeof(h), 1, fp) != 1 || memcmp(h.magic, kStateMagic, 8) != 0 ||
+      h.version != 1) {
+    fclose(fp);
+    return fail(LBM_ERR_ARG, "lbm_load_state: %s is not a liblbmb200 state file", path);
+  }
+  if (h.nx != s->nx || h.ny != s->ny || h.nz != s->nz || h.fluid_cells != s->n_fluid ||
+      h.pattern != s->pattern || h.steps_done < 0) {
+    fclose(fp);
+    return fail(LBM_ERR_ARG, "lbm_load_state: %s holds a %dx%dx%d state with %lld fluid cells "
+        "of pattern %d; the solver is %dx%dx%d with %lld fluid cells, pattern %d", path, h.nx,
+        h.ny, h.nz, (long long)h.fluid_cells, h.pattern, s->nx, s->ny, s->nz, s->n_fluid,
+        s->pattern);
+  }
+  std::vector<double> f;
+  try {
+    f.resize((size_t)Q * s->nx * s->ny * s->nz);
+  } catch (...) {
+    fclose(fp);
+    return fail(LBM_ERR_ALLOC, "lbm_load_state: host allocation failed");
+  }
+  const bool ok = fread(f.data(), sizeof(double), f.size(), fp) == f.size();
+  fclose(fp);
+  if (!ok)
+    return fail(LBM_ERR_ARG, "lbm_load_state: %s is truncated", path);
+  // the step count fixes the AA orientation the state is written in
+  const long long saved = s->steps_done;
+  s->steps_done = h.steps_done;
+  int rc = lbm_set_state(s, f.data());
+  if (rc)
+    s->steps_done = saved;
+  return rc;
+}
+
+// ---------------------------------------------------------------------------
 // Transfers in the reference's own padded layout (for the drop-in kernels)
 // ---------------------------------------------------------------------------
 

@@ -74,6 +74,8 @@ _SIGNATURES = [
     ("lbm_set_fp16_scale", ctypes.c_int, [_vp, ctypes.c_double]),
     ("lbm_set_porosity", ctypes.c_int, [_vp, _fp, ctypes.c_double]),
     ("lbm_set_state", ctypes.c_int, [_vp, _dp]),
+    ("lbm_save_state", ctypes.c_int, [_vp, ctypes.c_char_p]),
+    ("lbm_load_state", ctypes.c_int, [_vp, ctypes.c_char_p]),
     ("lbm_get_state", ctypes.c_int, [_vp, _dp]),
     ("lbm_run", ctypes.c_int, [_vp, ctypes.c_int]),
     ("lbm_synchronize", ctypes.c_int, [_vp]),
@@ -298,6 +300,14 @@ class Solver:
             raise ValueError("out must be a C-contiguous float64 array of the state's shape")
         _check(lib().lbm_get_state(self._h, _p(out, _dp)))
         return out
+
+    def save_state(self, path: str) -> None:
+        """Checkpoint: the state and the step count to a file (lbm_save_state)."""
+        _check(lib().lbm_save_state(self._h, os.fsencode(path)))
+
+    def load_state(self, path: str) -> None:
+        """Resume from a file written by save_state (lbm_load_state)."""
+        _check(lib().lbm_load_state(self._h, os.fsencode(path)))
 
     # -- stepping ----------------------------------------------------------
     def run(self, steps: int):

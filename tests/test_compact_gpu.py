@@ -239,3 +239,51 @@ def test_compact_full_size_equals_dense_bitwise():
         c = run(flags, (1, 0, 0), f0, 20, 1.25, 3 / 16, 1e-6, True, pattern)
         assert np.array_equal(c[:, m], dense[:, m]), pattern
         del c
+
+
+@pytest.mark.parametrize("precision", [L.F64, L.F32, L.F16])
+@pytest.mark.parametrize("pattern", PATTERNS)
+@pytest.mark.parametrize("compact", [False, True], ids=["dense", "compact"])
+def test_checkpoint_resume_is_bit_identical(tmp_path, pattern, precision, compact):
+    """lbm_save_state after 7 steps (AA: an odd count, so the state is in the
+    even-step orientation), then 6 more steps; a fresh solver that loads the
+    file and runs the same 6 steps ends in the same state, bit for bit, in
+    either layout (the file does not depend on it)."""
+    flags, _, _ = L.porous_channel((20, 18, 36), 0.2, 2.0, 4.0, seed=12)
+    f0 = L.perturbed_equilibrium(flags, seed=3, amplitude=1e-3)
+    path = str(tmp_path / "state.lbm")
+    with L.Solver(flags, (1, 0, 0), pattern, precision, compact=compact) as s:
+        s.set_params(1.2, 3 / 16, 1e-6, True)
+        s.set_state(f0)
+        s.run(7)
+        s.save_state(path)
+        s.run(6)
+        want = s.get_state()
+    with L.Solver(flags, (1, 0, 0), pattern, precision, compact=not compact) as r:
+        r.set_params(1.2, 3 / 16, 1e-6, True)
+        r.load_state(path)
+        assert r.steps_done == 7
+        r.run(6)
+        got = r.get_state()
+    assert np.array_equal(got, want)
+
+
+def test_checkpoint_rejects_other_geometry(tmp_path):
+    flags, _, _ = L.porous_channel((16, 24, 28), 0.25, 2.0, 3.0, seed=1)
+    other, _, _ = L.porous_channel((16, 24, 28), 0.25, 2.0, 3.0, seed=2)
+    assert (flags != 0).sum() != (other != 0).sum()
+    path = str(tmp_path / "a.lbm")
+    with L.Solver(flags, (1, 0, 0), "aa", L.F64) as s:
+        s.init_equilibrium(seed=1)
+        s.save_state(path)
+    with L.Solver(other, (1, 0, 0), "aa", L.F64) as r:
+        with pytest.raises(L.LbmError, match="fluid cells"):
+            r.load_state(path)
+    with L.Solver(flags, (1, 0, 0), "pull", L.F64) as r:
+        with pytest.raises(L.LbmError, match="pattern"):
+            r.load_state(path)
+    bad = tmp_path / "bad.lbm"
+    bad.write_bytes(b"not a state file")
+    with L.Solver(flags, (1, 0, 0), "aa", L.F64) as r:
+        with pytest.raises(L.LbmError, match="not a liblbmb200 state file"):
+            r.load_state(str(bad))
