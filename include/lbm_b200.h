@@ -92,6 +92,16 @@ int lbm_create_compact(lbm_solver **out, int nx, int ny, int nz, const int *flag
 /* 1 if the solver uses the compact layout, 0 if not, -1 for NULL. */
 int lbm_is_compact(const lbm_solver *s);
 
+/* The compact layout's index, built on the host (no GPU needed): fluid is
+ * rows x pitch bytes (nonzero = fluid, z fastest, the first nz of each row
+ * used). For each row and each 32-cell word w (W = (nz + 31) / 32 words per
+ * row) bits[r*W + w] gets one bit per fluid z and base[r*W + w] the number
+ * of fluid cells before it in row order, so the fluid cell (r, z) is stored
+ * at base + popcount(bits & bits below z). *total gets the fluid count.
+ * No counterpart in the reference. */
+int lbm_compact_index(const unsigned char *fluid, long long rows, int nz, int pitch,
+    unsigned int *bits, unsigned int *base, unsigned long long *total);
+
 /* Frees everything the solver owns (src/lbm.c:660-670). NULL is a no-op. */
 int lbm_destroy(lbm_solver *s);
 

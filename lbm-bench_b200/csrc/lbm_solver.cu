@@ -104,6 +104,30 @@ int lbm::record_error(int code, const char *fmt, ...)
   return code;
 }
 
+extern "C" int lbm_compact_index(const unsigned char *fluid, long long rows, int nz, int pitch,
+    unsigned int *bits, unsigned int *base, unsigned long long *total)
+{
+  if (!fluid || !bits || !base || rows < 0 || nz <= 0 || pitch < nz)
+    return fail(LBM_ERR_ARG, "lbm_compact_index: bad arguments");
+  const int W = (nz + 31) / 32;
+  unsigned long long run = 0;
+  for (long long r = 0; r < rows; ++r)
+    for (int w = 0; w < W; ++w) {
+      uint32_t word = 0;
+      for (int b = 0; b < 32 && 32 * w + b < nz; ++b)
+        word |= (uint32_t)(fluid[r * pitch + 32 * w + b] != 0) << b;
+      bits[r * W + w] = word;
+      base[r * W + w] = (uint32_t)run;
+      run += (unsigned long long)__builtin_popcount(word);
+    }
+  if (run >= (1ull << 32))
+    return fail(LBM_ERR_ARG, "lbm_compact_index: %llu fluid cells exceed the 32-bit numbering",
+        run);
+  if (total)
+    *total = run;
+  return LBM_OK;
+}
+
 extern "C" int lbm_device_count(void)
 {
   int n = 0;
@@ -664,16 +688,10 @@ static int create_impl(lbm_solver **out, int nx, int ny, int nz, const int *flag
     const size_t rows = (size_t)s->g.nx * s->g.ny;
     hbits.assign(rows * W, 0u);
     hbase.assign(rows * W, 0u);
-    uint32_t run = 0;
-    for (size_t r = 0; r < rows; ++r)
-      for (int w = 0; w < W; ++w) {
-        uint32_t bits = 0;
-        for (int b = 0; b < 32 && 32 * w + b < s->g.nz; ++b)
-          bits |= (uint32_t)fluid[r * s->g.pz + 32 * w + b] << b;
-        hbits[r * W + w] = bits;
-        hbase[r * W + w] = run;
-        run += (uint32_t)__builtin_popcount(bits);
-      }
+    unsigned long long total = 0;
+    lbm_compact_index(fluid.data(), (long long)rows, s->g.nz, s->g.pz, hbits.data(), hbase.data(),
+        &total);
+    const uint32_t run = (uint32_t)total;
     s->g.W = W;
     s->cplane0 = new std::vector<uint32_t>((size_t)s->g.nx + 1);
     for (int x = 0; x < s->g.nx; ++x)

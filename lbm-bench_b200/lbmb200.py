@@ -51,6 +51,8 @@ _SIGNATURES = [
                                           ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("lbm_is_compact", ctypes.c_int, [_vp]),
+    ("lbm_compact_index", ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                         _vp, _vp, ctypes.POINTER(ctypes.c_ulonglong)]),
     ("lbm_create_slab_compact", ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int,
                                                ctypes.c_int, _ip, ctypes.c_int, ctypes.c_int,
                                                ctypes.c_int, ctypes.c_int]),
@@ -426,6 +428,22 @@ def porous_channel(dims, solid_fraction=0.2, rmin=4.0, rmax=8.0, seed=42):
     _check(lib().lbm_porous_channel(nx, ny, nz, solid_fraction, rmin, rmax, seed,
                                     _p(flags, _ip), ctypes.byref(frac), ctypes.byref(n)))
     return flags, frac.value, n.value
+
+
+def compact_index(fluid, nz=None):
+    """The compact layout's index (lbm_compact_index) of fluid[rows, pitch]
+    (bool/uint8, the first nz entries of each row used): returns
+    (bits[rows, W], base[rows, W], total) as uint32 arrays and an int."""
+    fluid = np.ascontiguousarray(fluid, dtype=np.uint8)
+    rows, pitch = fluid.shape
+    nz = pitch if nz is None else nz
+    W = (nz + 31) // 32
+    bits = np.zeros((rows, W), dtype=np.uint32)
+    base = np.zeros((rows, W), dtype=np.uint32)
+    total = ctypes.c_ulonglong(0)
+    _check(lib().lbm_compact_index(fluid.ctypes.data, rows, nz, pitch, bits.ctypes.data,
+                                   base.ctypes.data, ctypes.byref(total)))
+    return bits, base, int(total.value)
 
 
 def perturbed_equilibrium(flags, seed=1, amplitude=1e-4, rho=1.0):

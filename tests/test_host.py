@@ -129,3 +129,64 @@ def test_oracle_workload_equals_product_generator(dims, frac, rmin, rmax, seed):
     f = L.perturbed_equilibrium(flags, seed=7, amplitude=1e-4)
     fo = O.counter_equilibrium(oflags, 7, 1e-4)
     assert f.tobytes() == fo.tobytes()
+
+
+def _rank(fluid):
+    """Storage number of every cell in row order (fluid cells only; -1 else)."""
+    flat = fluid.reshape(-1).astype(bool)
+    num = np.cumsum(flat) - 1
+    return np.where(flat, num, -1).reshape(fluid.shape)
+
+
+@pytest.mark.parametrize("rows,nz,pitch,seed", [(7, 45, 48, 1), (5, 32, 32, 2), (3, 96, 112, 3),
+                                                (11, 1, 16, 4), (4, 70, 80, 5)])
+def test_compact_index_words_and_bases(rows, nz, pitch, seed):
+    """lbm_compact_index: one fluid bit per z, and per 32-cell word the
+    number of fluid cells before it in row order; row padding beyond nz is
+    ignored."""
+    rng = np.random.default_rng(seed)
+    fluid = rng.uniform(size=(rows, pitch)) > 0.3
+    bits, base, total = L.compact_index(fluid, nz)
+    f = fluid[:, :nz]
+    assert total == int(f.sum())
+    rank = _rank(f)
+    for r in range(rows):
+        for z in range(nz):
+            w, b = divmod(z, 32)
+            assert bool((int(bits[r, w]) >> b) & 1) == bool(f[r, z])
+            if f[r, z]:
+                below = int(bits[r, w]) & ((1 << b) - 1)
+                assert int(base[r, w]) + bin(below).count("1") == rank[r, z]
+
+
+def test_compact_neighbour_identities():
+    """The step kernels find a fluid neighbour (row q, z + dz) of a lane at
+    z from row q's word at z alone: B_q = base + popc(word & bits below z),
+    f_q = bit z; (q, z) -> B_q, (q, z + 1) -> B_q + f_q, (q, z - 1) -> B_q - 1.
+    Checked here for every fluid cell and D3Q19 neighbour of a random box,
+    x and y periodic (rows wrap), z not (no wrap needed), nz = 70 so the
+    z +- 1 neighbours cross word boundaries."""
+    rng = np.random.default_rng(9)
+    nx, ny, nz = 6, 5, 70
+    fluid = rng.uniform(size=(nx, ny, nz)) > 0.35
+    bits, base, _ = L.compact_index(fluid.reshape(nx * ny, nz), nz)
+    rank = _rank(fluid)
+    checked = 0
+    for x in range(nx):
+        for y in range(ny):
+            for z in range(nz):
+                if not fluid[x, y, z]:
+                    continue
+                w, b = divmod(z, 32)
+                for d in range(19):
+                    xx, yy, zz = (x + O.CX[d]) % nx, (y + O.CY[d]) % ny, z + O.CZ[d]
+                    if not (0 <= zz < nz) or not fluid[xx, yy, zz]:
+                        continue  # a wall: the mask says so, no index is needed
+                    row = xx * ny + yy
+                    word = int(bits[row, w])
+                    bq = int(base[row, w]) + bin(word & ((1 << b) - 1)).count("1")
+                    fq = (word >> b) & 1
+                    idx = bq + fq if O.CZ[d] > 0 else bq - 1 if O.CZ[d] < 0 else bq
+                    assert idx == rank[xx, yy, zz], (x, y, z, d)
+                    checked += 1
+    assert checked > 10000
