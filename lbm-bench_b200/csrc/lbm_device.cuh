@@ -174,22 +174,22 @@ __device__ __forceinline__ void collide(const V (&f)[Q], V (&o)[Q], const Consts
 // to sit in (as in the reference's obstacle and ghost slots,
 // src/lbm.c:532-566).
 //
-// Compact ("fluid-only") layout, when `bits` is set: only fluid cells hold
+// Compact ("fluid-only") layout, when `wb` is set: only fluid cells hold
 // storage. The fluid cells of one (x, y) row sit consecutively in z order,
 // rows follow in (x, y) order, and a cell's storage index is its rank among
-// all fluid cells. Per row, W 32-bit words hold one fluid bit per z (bit
-// z % 32 of word z / 32), and base[] holds for every word the index of the
-// first fluid cell at or after z = 32 w, so a fluid cell's index is
-// base + popc(word & bits below z). Plane stride and mask array then count
-// fluid cells only; no solid cell shares a 32-byte sector with a fluid one.
+// all fluid cells. Per row, W pairs (word, base): `word` holds one fluid bit
+// per z (bit z % 32 of pair z / 32), `base` the index of the first fluid
+// cell at or after z = 32 w, so a fluid cell's index is
+// base + popc(word & bits below z); one 8-byte load fetches both. Plane
+// stride and mask array then count fluid cells only; no solid cell shares a
+// 32-byte sector with a fluid one.
 struct Grid {
   int nx, ny, nz;  // device extent (the caller's box plus frames)
   int pz;          // z pitch of a row, elements
   int per;         // periodic axes: bit 0 x, bit 1 y, bit 2 z
   long long plane; // elements per direction plane
-  const uint32_t *bits = nullptr; // compact layout: fluid bits [nx*ny rows][W]
-  const uint32_t *base = nullptr; // compact layout: first index at or after each word
-  int W = 0;                      // compact layout: words per row
+  const uint2 *wb = nullptr; // compact layout: (fluid bits, first index) [nx*ny rows][W]
+  int W = 0;                 // compact layout: words per row
 };
 
 // Caller's box inside the device box: offsets and extent.
@@ -250,7 +250,8 @@ __device__ __forceinline__ uint32_t packed_index(const Grid &g, int x, int y, in
 {
   const uint32_t k =
       ((uint32_t)x * (uint32_t)g.ny + (uint32_t)y) * (uint32_t)g.W + (uint32_t)(z >> 5);
-  return __ldg(g.base + k) + (uint32_t)__popc(__ldg(g.bits + k) & ((1u << (z & 31)) - 1u));
+  const uint2 wb = __ldg(g.wb + k);
+  return wb.y + (uint32_t)__popc(wb.x & ((1u << (z & 31)) - 1u));
 }
 
 // Storage index and link mask of the device cell (x, y, z) in either
@@ -259,13 +260,13 @@ __device__ __forceinline__ uint32_t packed_index(const Grid &g, int x, int y, in
 __device__ __forceinline__ bool locate(const Grid &g, const uint32_t *mask, int x, int y, int z,
     uint32_t &cell, uint32_t &m)
 {
-  if (g.bits) {
+  if (g.wb) {
     const uint32_t k =
         ((uint32_t)x * (uint32_t)g.ny + (uint32_t)y) * (uint32_t)g.W + (uint32_t)(z >> 5);
-    const uint32_t w = __ldg(g.bits + k);
-    if (!((w >> (z & 31)) & 1u))
+    const uint2 wb = __ldg(g.wb + k);
+    if (!((wb.x >> (z & 31)) & 1u))
       return false;
-    cell = __ldg(g.base + k) + (uint32_t)__popc(w & ((1u << (z & 31)) - 1u));
+    cell = wb.y + (uint32_t)__popc(wb.x & ((1u << (z & 31)) - 1u));
   } else {
     cell = cell_index(g, x, y, z);
   }
@@ -283,7 +284,7 @@ struct Nbr {
   const Grid *g;
   __device__ __forceinline__ uint32_t at(int d) const
   {
-    if (!g->bits)
+    if (!g->wb)
       return cell + o.at(d);
     int a = x + cx(d), b = y + cy(d), c = z + cz(d);
     a = a < 0 ? g->nx - 1 : a >= g->nx ? 0 : a;

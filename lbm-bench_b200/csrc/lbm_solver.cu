@@ -89,7 +89,7 @@ struct lbm_solver {
   int split_left;        // planes still to launch
   // compact (fluid-only) layout: fluid bits and word bases per row (Grid)
   int compact;
-  uint32_t *cbits, *cbase;
+  uint2 *cwb; // compact layout: (fluid bits, first index) per row word
   std::vector<uint32_t> *cplane0; // storage index of the first fluid cell of each x plane (nx+1)
 };
 
@@ -541,8 +541,7 @@ static void free_all(lbm_solver *s)
   cudaFree(s->red);
   cudaFree(s->dev_err);
   cudaFree(s->bc_marks);
-  cudaFree(s->cbits);
-  cudaFree(s->cbase);
+  cudaFree(s->cwb);
   delete s->cplane0;
   free(s->split_done);
   if (s->fork_ev)
@@ -795,16 +794,15 @@ static int create_impl(lbm_solver **out, int nx, int ny, int nz, const int *flag
   // the fluid cells' storage indices
   if (s->compact) {
     const size_t nw = hbits.size() * sizeof(uint32_t);
-    TRY(dev_alloc(s, (void **)&s->cbits, nw, "the compact layout's fluid bits"));
-    TRY(dev_alloc(s, (void **)&s->cbase, nw, "the compact layout's word bases"));
-    TRYC(cudaMemcpy(s->cbits, hbits.data(), nw, cudaMemcpyHostToDevice));
-    TRYC(cudaMemcpy(s->cbase, hbase.data(), nw, cudaMemcpyHostToDevice));
-    s->g.bits = s->cbits;
-    s->g.base = s->cbase;
+    std::vector<uint2> hwb(hbits.size());
+    for (size_t k = 0; k < hwb.size(); ++k)
+      hwb[k] = make_uint2(hbits[k], hbase[k]);
+    TRY(dev_alloc(s, (void **)&s->cwb, 2 * nw, "the compact layout's index"));
+    TRYC(cudaMemcpy(s->cwb, hwb.data(), 2 * nw, cudaMemcpyHostToDevice));
+    s->g.wb = s->cwb;
   }
   Grid gd = s->g; // dense view of the box for the mask build
-  gd.bits = nullptr;
-  gd.base = nullptr;
+  gd.wb = nullptr;
   const long long dense_plane = (cells + pq - 1) / pq * pq;
   uint32_t *dmask = s->mask;
   if (s->compact)
@@ -1921,12 +1919,12 @@ __global__ void halo_copy_kernel(Grid g, UserBox u, int xplane, int sgn, T *stat
   const int d = halo_dir(sgn, k);
   const size_t bi = ((size_t)k * u.ny + y) * u.nz + z;
   uint32_t cell;
-  if (g.bits) {
+  if (g.wb) {
     // compact layout: only stored (fluid) cells take part; a solid cell
     // sends 0 and receives nothing
     const uint32_t wk = ((uint32_t)xplane * (uint32_t)g.ny + (uint32_t)(y + u.oy)) *
         (uint32_t)g.W + (uint32_t)((z + u.oz) >> 5);
-    if (!((g.bits[wk] >> ((z + u.oz) & 31)) & 1u)) {
+    if (!((g.wb[wk].x >> ((z + u.oz) & 31)) & 1u)) {
       if (to_buf)
         buf[bi] = T(0);
       return;

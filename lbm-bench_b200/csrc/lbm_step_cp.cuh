@@ -16,8 +16,8 @@
 // solid lane leaves after one fluid-bit test. Because a warp's lanes share
 // the row and the fluid-bit word, the storage index of a fluid cell and of
 // its neighbours comes from nine warp-uniform word pairs (own row and the
-// eight rows (x +- 1, y +- 1)): with B_q = base + popc(word_q & bits below
-// z) and f_q the fluid bit of (row q, z),
+// eight rows (x +- 1, y +- 1), one 8-byte load each): with B_q = base +
+// popc(word_q & bits below z) and f_q the fluid bit of (row q, z),
 //     index of (row q, z)     = B_q
 //     index of (row q, z + 1) = B_q + f_q      (when that cell is fluid)
 //     index of (row q, z - 1) = B_q - 1        (when that cell is fluid)
@@ -32,27 +32,38 @@
 
 namespace lbm {
 
-// Register caps of the compact kernels (minimum CTAs per SM), per kind from
-// a sweep on the 256^3 porous channel (B200): AA odd and pull are fastest
-// at 8 CTAs/SM (64 registers; odd 0.963 ms at 6 with the row table in
-// registers, 0.803 at 6 and 0.764 at 8 with it in shared memory), push at 7,
-// the local AA even step (at the HBM limit) does not care.
+// Register caps of the compact kernels (minimum CTAs per SM), per kind and
+// storage width from sweeps on the 256^3 porous channel (B200): AA odd and
+// pull are fastest at 8 CTAs/SM (64 registers; FP64 odd 0.963 ms at 6 with
+// the row table in registers, 0.803 at 6 and 0.764 at 8 with it in shared
+// memory); push at 6 for FP64 (0.751 ms; 0.768 at 7, 0.918 at 8), 8 for
+// FP16 (0.364 ms; 0.374 at 7, 0.395 at 6) and 8 for FP32 (0.439 ms; 0.458
+// at 7); the local AA even step (at the HBM limit) does not care.
 #ifndef LBM_MINB_CP_ODD
 #define LBM_MINB_CP_ODD 8
 #endif
 #ifndef LBM_MINB_CP_PULL
 #define LBM_MINB_CP_PULL 8
 #endif
-#ifndef LBM_MINB_CP_PUSH
-#define LBM_MINB_CP_PUSH 7
+#ifndef LBM_MINB_CP_PUSH_F64
+#define LBM_MINB_CP_PUSH_F64 6
+#endif
+#ifndef LBM_MINB_CP_PUSH_F32
+#define LBM_MINB_CP_PUSH_F32 8
+#endif
+#ifndef LBM_MINB_CP_PUSH_F16
+#define LBM_MINB_CP_PUSH_F16 8
 #endif
 #ifndef LBM_MINB_CP_EVEN
 #define LBM_MINB_CP_EVEN 6
 #endif
-template <int KIND> struct CpOccupancy {
+// SB: bytes of one stored population (8, 4 or 2).
+template <int KIND, int SB> struct CpOccupancy {
+  static constexpr int push = SB == 8 ? LBM_MINB_CP_PUSH_F64
+      : SB == 4 ? LBM_MINB_CP_PUSH_F32 : LBM_MINB_CP_PUSH_F16;
   static constexpr int value = KIND == kAAEvenStep ? LBM_MINB_CP_EVEN
       : KIND == kAAOddStep ? LBM_MINB_CP_ODD
-      : KIND == kPullStep ? LBM_MINB_CP_PULL : LBM_MINB_CP_PUSH;
+      : KIND == kPullStep ? LBM_MINB_CP_PULL : push;
 };
 
 // Storage indices of the 18 neighbours of one fluid cell (compact layout).
@@ -96,8 +107,9 @@ template <bool ZPER> struct RowTab {
       xr = xr < 0 ? g.nx - 1 : xr >= g.nx ? 0 : xr;
       yr = yr < 0 ? g.ny - 1 : yr >= g.ny ? 0 : yr;
       const uint32_t k = ((uint32_t)xr * (uint32_t)g.ny + (uint32_t)yr) * (uint32_t)g.W + wi;
-      const uint32_t w = __ldg(g.bits + k);
-      B[q] = __ldg(g.base + k) + (uint32_t)__popc(w & lt);
+      const uint2 wb = __ldg(g.wb + k);
+      const uint32_t w = wb.x;
+      B[q] = wb.y + (uint32_t)__popc(w & lt);
       if (q == 1 || q == 3 || q == 5 || q == 7)
         B[axis_slot(q)] = B[q] + ((w >> lane) & 1u);
     }
@@ -155,7 +167,7 @@ template <class ST> struct CpMathDirect {
 // OFF: type of element offsets within the state (uint32_t when all 19
 // planes fit below 2^32 elements, which keeps address arithmetic 32-bit).
 template <class M, int KIND, bool FORCE, bool ZPER, typename OFF>
-__global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND>::value))
+__global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND, sizeof(typename M::S)>::value))
     step_kernel_cp(typename M::Args a)
 {
   using S = typename M::S;
@@ -171,10 +183,11 @@ __global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND>::value))
   const uint32_t lt = (1u << lane) - 1u;
   const uint32_t wi = (uint32_t)(z >> 5);
   const uint32_t k0 = ((uint32_t)x * (uint32_t)g.ny + (uint32_t)y) * (uint32_t)g.W + wi;
-  const uint32_t w0 = __ldg(g.bits + k0);
+  const uint2 wb0 = __ldg(g.wb + k0);
+  const uint32_t w0 = wb0.x;
   if (!((w0 >> lane) & 1u))
     return;
-  const uint32_t cell = __ldg(g.base + k0) + (uint32_t)__popc(w0 & lt);
+  const uint32_t cell = wb0.y + (uint32_t)__popc(w0 & lt);
   const uint32_t mask = __ldg(a.mask + cell);
   const S *src = a.src;
   S *dst = a.dst;
@@ -241,7 +254,7 @@ __global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND>::value))
 // index lookup in front of them. Only the link mask (bounce-back force
 // direction) is read besides the populations.
 template <class ST, bool FORCE>
-__global__ void __launch_bounds__(kStepThreads, (CpOccupancy<kAAEvenStep>::value))
+__global__ void __launch_bounds__(kStepThreads, (CpOccupancy<kAAEvenStep, sizeof(typename ST::S)>::value))
     step_kernel_cp_local(StepArgs<ST> a)
 {
   using S = typename ST::S;
