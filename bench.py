@@ -372,6 +372,8 @@ def run_native(args, dist: Dist):
     }
     s.close()
     if not args.no_studies:
+        result["ring_1gpu"] = ring_study(L, flags, f0, args.steps, args.warmup, ms / args.steps,
+                                         compact)
         result["precision_512"] = precision_study(L, 512, 300, peak)
         result["largest"] = largest_study(L, 768, 200, peak)
     if not args.no_parity:
@@ -454,6 +456,10 @@ def summary(r):
         out["parity"] = {c: {"rho": _r(q[c]["max_rel_err_rho"], 3), "u": _r(q[c]["max_rel_err_u"], 3),
                              "bitwise": q[c]["bit_identical"], "steps": q[c]["steps"]}
                          for c in ("config0", "config1")}
+    g = r.get("ring_1gpu")
+    if g:
+        out["ring_1gpu"] = {k: {"ms": _r(g[k]["ms_per_step"]), "overhead": _r(g[k]["overhead"], 3)}
+                            for k in ("native_nccl", "native_copy", "python_copy")}
     out["e2e_mlups"] = _r(r["e2e"]["value"])
     if "transfer_gbs" in r["e2e"]:
         out["e2e_transfer_gbs"] = _r(r["e2e"]["transfer_gbs"], 3)
@@ -760,11 +766,62 @@ def run_largest(args):
                      "f32 (f16 storage)", res)
 
 
+def ring_study(L, flags, f0, steps: int, warmup: int, plain_ms: float, compact: bool):
+    """The halo-exchange data plane on one GPU: the x-periodic channel as one
+    x-slab that is its own neighbour, FP64 AA, overlapped schedule. Three
+    transports: the native ring through a one-rank NCCL communicator (send
+    and receive to itself: the NCCL path of a multi-GPU run without a peer),
+    the native ring with device copies, and the Python-driven SlabRunner.
+    Device time with CUDA events on the solver's stream; `overhead` is the
+    step time against the undecomposed solver's (plain_ms per step)."""
+    import lbm_slab
+    import torch
+
+    out = {"workload": f"{flags.shape[2]}x{flags.shape[1]}x{flags.shape[0]} channel as one "
+                       "x-slab, FP64 AA, ghost planes exchanged every odd step",
+           "undecomposed_ms_per_step": plain_ms}
+    for name in ("native_nccl", "native_copy", "python_copy"):
+        s = L.Solver.slab(lbm_slab.slab_flags(flags, 0, flags.shape[2]), (0, 0), "aa", L.F64,
+                          compact=compact)
+        s.set_params(1.25, 3 / 16, 1e-6, True)
+        s.set_state(f0)
+        if name.startswith("native"):
+            r = lbm_slab.NativeRunner(s, overlap=True, nccl=name == "native_nccl")
+        else:
+            r = lbm_slab.SlabRunner(s, lbm_slab.Ring(), overlap=True)
+        r.scatter()
+        r.run(warmup)
+        s.synchronize()
+        ext = torch.cuda.ExternalStream(s.stream)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ex0, l0 = r.exchanges, s.launch_count
+        t0 = time.perf_counter()
+        ev0.record(ext)
+        r.run(steps)
+        ev1.record(ext)
+        issue = time.perf_counter() - t0
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        out[name] = {"ms_per_step": ms / steps, "mlups": s.fluid_cells * steps / (ms / 1e3) / 1e6,
+                     "overhead": ms / steps / plain_ms - 1, "exchanges": r.exchanges - ex0,
+                     "step_launches": s.launch_count - l0,
+                     "host_issue_ms_per_step": issue * 1e3 / steps}
+        r.gather()
+        tot, bad = s.mass_momentum(check=False)
+        out[name]["nonfinite_cells"] = bad
+        if hasattr(r, "close"):
+            r.close()
+        s.close()
+    return out
+
+
 def run_slabs(args, dist: Dist):
     """N GPUs: the porous channel of N x 256 x 256 x 256 cells cut into one
     256^3 x-slab per rank (weak scaling), FP64 AA, halo exchange between
     ring neighbours over NCCL every odd step, overlapped with the update of
-    the interior planes (lbm_slab.SlabRunner(overlap=True))."""
+    the interior planes. The step loop and the NCCL send/recv are issued by
+    the library (lbm_ring_run through lbm_slab.NativeRunner), not by Python
+    per step."""
     import lbm_slab
     import lbmb200 as L
     import numpy as np
@@ -782,7 +839,8 @@ def run_slabs(args, dist: Dist):
     s = L.Solver.slab(sflags, (0, 0), "aa", L.F64, compact=args.layout == "compact")
     s.set_params(1.25, 3 / 16, 1e-6, True)
     s.set_state(f0)
-    runner = lbm_slab.SlabRunner(s, lbm_slab.Ring(), overlap=True)
+    runner = lbm_slab.NativeRunner(s, overlap=True, timeout_ms=120000)
+    ext = torch.cuda.ExternalStream(s.stream)
     runner.scatter()
     n_fluid = s.fluid_cells
     bpu = s.bytes_per_update
@@ -793,14 +851,15 @@ def run_slabs(args, dist: Dist):
     dist.barrier()
     s.synchronize()
     with ClockSampler(dist.local) as clk:
-        ev0.record(runner.ext)
+        ev0.record(ext)
         runner.run(args.steps)
-        ev1.record(runner.ext)
+        ev1.record(ext)
         ev1.synchronize()
     dist.barrier()
     ms = dist.max(ev0.elapsed_time(ev1))
     total_fluid = dist.sum(float(n_fluid))
-    launches = (s.launch_count - launches0) + 4 * (runner.exchanges - ex0)
+    # per exchange: the pack kernel, NCCL's grouped send/recv kernel, the unpack kernel
+    launches = (s.launch_count - launches0) + 3 * (runner.exchanges - ex0)
     runner.gather()
     tot, bad = s.mass_momentum(check=False)
     mass = dist.sum(tot[0])
@@ -825,8 +884,9 @@ def run_slabs(args, dist: Dist):
     e2e = {"value": total_fluid * args.steps / t / 1e6, "unit": "MLUPS",
            "h2d_bytes_per_step": f0.nbytes / args.steps,
            "d2h_bytes_per_step": host.nbytes / args.steps, "seconds": t,
-           "call": "lbm_set_state (pinned host) + SlabRunner.run (steps + NCCL halo exchange) + "
+           "call": "lbm_set_state (pinned host) + lbm_ring_run (steps + NCCL halo exchange) + "
                    "lbm_get_state, per rank"}
+    runner.close()
     s.close()
     return {
         "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world,
@@ -839,8 +899,9 @@ def run_slabs(args, dist: Dist):
                        fluid_cells=int(total_fluid), parallelism=f"x-slabs x{world}",
                        layout=args.layout,
                        halo="5 populations x 256 x 256 per face, before and after each odd "
-                            "AA step, NCCL send/recv between ring neighbours, overlapped with "
-                            "the interior planes' update on a second stream"),
+                            "AA step, NCCL send/recv between ring neighbours issued from C "
+                            "(lbm_ring_run), overlapped with the interior planes' update on a "
+                            "second stream"),
         "gbs": achieved * world,
         "roofline": {"bound": "hbm", "kernel": "step_kernel<StoreF64> AA even+odd with halo "
                                                "exchange (whole step, per GPU)",

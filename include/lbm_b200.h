@@ -37,6 +37,8 @@ extern "C" {
 #define LBM_ERR_NONFINITE (-4) /* the state holds NaN or Inf */
 #define LBM_ERR_STATE (-5)     /* call not valid in the solver's current state */
 #define LBM_ERR_NODEV (-6)     /* no CUDA device (the product has no CPU path) */
+#define LBM_ERR_COMM (-7)      /* NCCL missing, or a communicator call failed */
+#define LBM_ERR_TIMEOUT (-8)   /* a bounded wait on a peer ran out; the communicator was aborted */
 
 /* Propagation patterns, numbered as the reference's PROP_* (src/lbm.h:148). */
 #define LBM_PUSH 0
@@ -219,6 +221,52 @@ void *lbm_stream(const lbm_solver *s);
 int lbm_step_begin(lbm_solver *s);
 int lbm_step_planes(lbm_solver *s, int x_begin, int x_end, int on_side);
 int lbm_step_end(lbm_solver *s);
+
+/* Native ring of x-slabs: the halo exchange of lbm_create_slab solvers
+ * between ring neighbours over NCCL point-to-point (send/recv of the
+ * lbm_halo_pack messages, ordered on the solver's stream), with the step
+ * loop - split steps, packs, transports, unpacks - issued from C, one ring
+ * per rank and GPU. No counterpart in the reference (LBM-Bench has no
+ * decomposition, src/main.c). NCCL is loaded when first needed (dlopen of
+ * libnccl.so.2, or of the file named by the environment variable
+ * LBM_B200_NCCL; a copy already loaded in the process is reused), so the
+ * library does not depend on it.
+ *
+ * lbm_ring_unique_id fills the 128-byte id that rank 0 creates and every
+ * rank passes to lbm_ring_create (broadcast it over any host channel); it
+ * needs no GPU. lbm_ring_create: rank in [0, nranks), the ring's left
+ * neighbour is rank - 1 and the right one rank + 1 (wrapped). With id NULL
+ * and nranks 1 the slab is its own neighbour on both sides (an x-periodic
+ * domain in one slab) and the messages move by device copies, without NCCL.
+ * Every wait on the communicator or on the stream - its creation, each
+ * exchange's group, lbm_ring_synchronize, and the run loop, which keeps at
+ * most 32 steps queued - gives up after timeout_ms (0: 60000), aborts the
+ * communicator (which ends NCCL kernels waiting for a peer) and returns
+ * LBM_ERR_TIMEOUT; after that, or after LBM_ERR_COMM, every call but
+ * lbm_ring_destroy returns LBM_ERR_STATE.
+ *
+ * lbm_ring_run enqueues `steps` steps with the exchanges that lbm_halo_needs
+ * asks for. overlap = 1 splits each step (lbm_step_begin/_planes/_end): the
+ * interior planes run on the solver's second stream while its own stream
+ * exchanges and updates the boundary planes. lbm_ring_gather and
+ * lbm_ring_scatter are the LBM_HALO_BEFORE / LBM_HALO_SCATTER exchanges that
+ * lbm_halo_shifted states need before reading and after setting the state.
+ * All ranks make the same calls in the same order. */
+typedef struct lbm_ring lbm_ring;
+#define LBM_RING_ID_BYTES 128
+int lbm_ring_unique_id(unsigned char *id);
+int lbm_ring_create(lbm_ring **out, lbm_solver *s, int rank, int nranks,
+    const unsigned char *id, int timeout_ms);
+int lbm_ring_run(lbm_ring *r, int steps, int overlap);
+int lbm_ring_gather(lbm_ring *r);
+int lbm_ring_scatter(lbm_ring *r);
+int lbm_ring_synchronize(lbm_ring *r);
+/* Exchanges issued so far (each one: a pack, one send and one receive per
+ * neighbour, an unpack); -1 for NULL. */
+long long lbm_ring_exchanges(const lbm_ring *r);
+/* 1 if the messages travel over NCCL, 0 for the device-copy ring of one. */
+int lbm_ring_uses_nccl(const lbm_ring *r);
+int lbm_ring_destroy(lbm_ring *r);
 
 /* Sets the state on the device to the seeded initial condition of
  * lbm_perturbed_equilibrium (identical values, no host array): for domains

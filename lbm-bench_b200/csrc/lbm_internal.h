@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include "lbm_b200.h"
+
 #include "lbm_adjoint.cuh"
 #include "lbm_step.cuh"
 #include "lbm_step_cp.cuh"
@@ -54,6 +56,11 @@ cudaError_t launch_adjoint_seed(int precision, const Grid &g, int xo, double inv
 
 // Records the message returned by lbm_last_error() and returns `code`.
 int record_error(int code, const char *fmt, ...);
+
+// The solver's own x planes (a slab's, without ghosts) and its CUDA device,
+// for host drivers in other translation units; -1 for NULL.
+int solver_planes(const lbm_solver *s);
+int solver_device(const lbm_solver *s);
 
 // Block/grid shape of the per-cell kernels: z across lanes, then y, one
 // x-plane per grid.z.

@@ -2082,6 +2082,9 @@ extern "C" int lbm_halo_unpack(lbm_solver *s, int when, const void *from_left,
 
 extern "C" void *lbm_stream(const lbm_solver *s) { return s ? (void *)s->stream : NULL; }
 
+int lbm::solver_planes(const lbm_solver *s) { return s ? s->nx : -1; }
+int lbm::solver_device(const lbm_solver *s) { return s ? s->device : -1; }
+
 // ---------------------------------------------------------------------------
 // Seeded initial state on the device
 // ---------------------------------------------------------------------------

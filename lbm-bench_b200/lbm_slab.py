@@ -13,10 +13,16 @@ The pull state, and the AA state after an odd number of steps, keep part of
 a boundary cell's populations in the neighbour's cells: call scatter() after
 setting slab states and gather() before reading them.
 
-Transport: torch.distributed point-to-point (NCCL over NVLink between GPUs,
-gloo between CPU processes), ordered on the solver's CUDA stream, so the
-exchange never blocks the host. `LocalRing` runs several slabs of one
-process (on one or several devices) with device copies instead.
+Transports:
+- `NativeRunner`: the ring in C (lbm_ring_* in include/lbm_b200.h, L.SlabRing):
+  NCCL send/recv between ring neighbours on the solver's stream and the whole
+  step loop issued by the library, so no Python runs per step. torch.distributed
+  only carries the NCCL id from rank 0 to the others once.
+- `SlabRunner` + `Ring`: the same schedule driven from Python over
+  torch.distributed point-to-point (NCCL between GPUs, gloo between CPU
+  processes); it also runs the numpy slab model of the tests.
+- `LocalRing`: several slabs of one process (on one or several devices) with
+  device copies.
 
 LBM-Bench itself has no decomposition (single-node OpenMP, src/main.c).
 """
@@ -174,6 +180,65 @@ class SlabRunner:
         in the ghost planes go to the neighbours (shifted states only)."""
         if self.s.halo_shifted:
             self._exchange(L.HALO_SCATTER)
+
+
+def share_ring_id(group=None):
+    """Rank 0 of the process group makes an NCCL id for lbm_ring_create
+    (L.ring_unique_id, no GPU needed) and broadcasts it; every rank returns
+    the same 128 bytes. None without a process group of two or more ranks."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size(group) == 1:
+        return None
+    obj = [L.ring_unique_id() if dist.get_rank(group) == 0 else None]
+    src = dist.get_global_rank(group, 0) if group is not None else 0
+    dist.broadcast_object_list(obj, src=src, group=group)
+    return obj[0]
+
+
+class NativeRunner:
+    """SlabRunner's schedule issued from C (L.SlabRing over lbm_ring_*): the
+    halo messages travel over NCCL between ring neighbours, ordered on the
+    solver's stream, and no Python runs per step. Ranks are those of the
+    process group (ring neighbours rank - 1 and rank + 1); with one rank the
+    slab is its own neighbour, by device copies or, with nccl=True, through
+    a one-rank NCCL communicator (sends to itself). All ranks construct it
+    together (the id broadcast is a collective)."""
+
+    def __init__(self, solver, group=None, overlap=True, timeout_ms=0, nccl=None):
+        import torch.distributed as dist
+        if dist.is_available() and dist.is_initialized():
+            rank, world = dist.get_rank(group), dist.get_world_size(group)
+        else:
+            rank, world = 0, 1
+        uid = share_ring_id(group)
+        if uid is None and nccl:
+            uid = L.ring_unique_id()
+        self.s = solver
+        self.overlap = overlap
+        self.ring = L.SlabRing(solver, rank, world, uid, timeout_ms)
+
+    @property
+    def exchanges(self) -> int:
+        return self.ring.exchanges
+
+    @property
+    def uses_nccl(self) -> bool:
+        return self.ring.uses_nccl
+
+    def run(self, steps: int) -> None:
+        self.ring.run(steps, self.overlap)
+
+    def gather(self) -> None:
+        self.ring.gather()
+
+    def scatter(self) -> None:
+        self.ring.scatter()
+
+    def synchronize(self) -> None:
+        self.ring.synchronize()
+
+    def close(self) -> None:
+        self.ring.close()
 
 
 class LocalRing:

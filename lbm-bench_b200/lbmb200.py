@@ -23,6 +23,8 @@ PUSH, PULL, AA = 0, 1, 2
 F64, F32, F16 = 0, 1, 2
 CKPT_AUTO = -1  # lbm_adjoint_gradient: least recomputation that fits in device memory
 HALO_BEFORE, HALO_AFTER, HALO_SCATTER = 1, 2, 4
+RING_ID_BYTES = 128
+ERR_COMM, ERR_TIMEOUT = -7, -8
 PATTERNS = {"push": PUSH, "pull": PULL, "aa": AA}
 PRECISIONS = {"fp64": F64, "fp32": F32, "fp16": F16}
 Q = 19
@@ -113,6 +115,16 @@ _SIGNATURES = [
     ("lbm_perturbed_equilibrium", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip,
                                                  ctypes.c_ulonglong, ctypes.c_double,
                                                  ctypes.c_double, _dp]),
+    ("lbm_ring_unique_id", ctypes.c_int, [_vp]),
+    ("lbm_ring_create", ctypes.c_int, [ctypes.POINTER(_vp), _vp, ctypes.c_int, ctypes.c_int, _vp,
+                                       ctypes.c_int]),
+    ("lbm_ring_run", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    ("lbm_ring_gather", ctypes.c_int, [_vp]),
+    ("lbm_ring_scatter", ctypes.c_int, [_vp]),
+    ("lbm_ring_synchronize", ctypes.c_int, [_vp]),
+    ("lbm_ring_exchanges", ctypes.c_longlong, [_vp]),
+    ("lbm_ring_uses_nccl", ctypes.c_int, [_vp]),
+    ("lbm_ring_destroy", ctypes.c_int, [_vp]),
 ]
 
 
@@ -393,6 +405,74 @@ class Solver:
     @property
     def launch_count(self) -> int:
         return lib().lbm_launch_count(self._h)
+
+
+def ring_unique_id() -> bytes:
+    """The 128-byte NCCL id of a new ring (lbm_ring_unique_id; no GPU
+    needed). Rank 0 makes it and every rank passes it to SlabRing."""
+    buf = ctypes.create_string_buffer(RING_ID_BYTES)
+    _check(lib().lbm_ring_unique_id(buf))
+    return buf.raw
+
+
+class SlabRing:
+    """The native ring of one slab solver (lbm_ring_* in
+    include/lbm_b200.h): halo messages to the ring neighbours over NCCL
+    (rank - 1 and rank + 1, wrapped), the step loop issued from C.
+
+    uid None with nranks 1: the slab is its own neighbour on both sides and
+    the messages move by device copies. Every wait on the communicator or
+    the stream is bounded by timeout_ms (0: 60 s); when one runs out the
+    communicator is aborted and the call raises LbmError(ERR_TIMEOUT)."""
+
+    def __init__(self, solver: Solver, rank: int = 0, nranks: int = 1, uid: bytes | None = None,
+                 timeout_ms: int = 0):
+        h = _vp()
+        idbuf = None
+        if uid is not None:
+            if len(uid) != RING_ID_BYTES:
+                raise ValueError(f"ring id must be {RING_ID_BYTES} bytes, got {len(uid)}")
+            idbuf = ctypes.create_string_buffer(bytes(uid), RING_ID_BYTES)
+        _check(lib().lbm_ring_create(ctypes.byref(h), solver._h, int(rank), int(nranks), idbuf,
+                                     int(timeout_ms)))
+        self._h = h
+        self.solver = solver
+        self.rank, self.nranks = int(rank), int(nranks)
+
+    def run(self, steps: int, overlap: bool = False) -> None:
+        """Enqueues `steps` steps with their exchanges (lbm_ring_run)."""
+        _check(lib().lbm_ring_run(self._h, int(steps), int(overlap)))
+
+    def gather(self) -> None:
+        """Before reading the slab's state (lbm_ring_gather)."""
+        _check(lib().lbm_ring_gather(self._h))
+
+    def scatter(self) -> None:
+        """After setting the slab's state (lbm_ring_scatter)."""
+        _check(lib().lbm_ring_scatter(self._h))
+
+    def synchronize(self) -> None:
+        _check(lib().lbm_ring_synchronize(self._h))
+
+    @property
+    def exchanges(self) -> int:
+        return lib().lbm_ring_exchanges(self._h)
+
+    @property
+    def uses_nccl(self) -> bool:
+        return lib().lbm_ring_uses_nccl(self._h) == 1
+
+    def close(self) -> None:
+        """Destroys the ring (before its solver)."""
+        if getattr(self, "_h", None):
+            h, self._h = self._h, None
+            _check(lib().lbm_ring_destroy(h))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def pin(a: np.ndarray) -> None:

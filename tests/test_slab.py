@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 import lbm_slab
+import lbmb200 as L
 import slab_model as M
 
 PATTERNS = ["pull", "push", "aa"]
@@ -172,3 +173,49 @@ def test_slab_runner_over_gloo_matches_periodic_run(pattern, world, overlap):
     ref = M.Periodic(fluid, pattern, f0)
     ref.run(steps)
     assert np.array_equal(got[:, fluid], ref.own_state()[:, fluid])
+
+
+# ---------------------------------------------------------------------------
+# native ring (lbm_ring_*): the NCCL id reaches every rank; argument checks
+# ---------------------------------------------------------------------------
+
+def _id_worker(rank, world, port, outdir):
+    import torch.distributed as dist
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world)
+    try:
+        uid = lbm_slab.share_ring_id()
+        with open(os.path.join(outdir, f"id{rank}.bin"), "wb") as f:
+            f.write(uid)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_ring_id_is_shared_by_all_ranks(world):
+    """Rank 0 makes the NCCL id (lbm_ring_unique_id, no GPU needed) and the
+    process group carries it once; every rank must hold the same bytes."""
+    import torch.multiprocessing as mp
+    with tempfile.TemporaryDirectory() as outdir:
+        mp.start_processes(_id_worker, args=(world, _free_port(), outdir), nprocs=world,
+                           join=True, start_method="spawn")
+        ids = [open(os.path.join(outdir, f"id{r}.bin"), "rb").read() for r in range(world)]
+    assert len(ids[0]) == L.RING_ID_BYTES and any(ids[0])
+    assert all(i == ids[0] for i in ids)
+
+
+def test_ring_id_without_process_group_is_none():
+    assert lbm_slab.share_ring_id() is None
+    a, b = L.ring_unique_id(), L.ring_unique_id()
+    assert len(a) == len(b) == L.RING_ID_BYTES and a != b
+
+
+def test_ring_create_rejects_bad_arguments_without_gpu():
+    import ctypes
+    h = ctypes.c_void_p()
+    lib = L.lib()
+    assert lib.lbm_ring_create(ctypes.byref(h), None, 0, 1, None, 0) == -1
+    assert lib.lbm_ring_exchanges(None) == -1 and lib.lbm_ring_uses_nccl(None) == -1
+    assert lib.lbm_ring_run(None, 1, 0) == -1
+    assert lib.lbm_ring_destroy(None) == 0
