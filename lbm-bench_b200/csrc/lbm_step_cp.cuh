@@ -33,17 +33,33 @@
 namespace lbm {
 
 // Register caps of the compact kernels (minimum CTAs per SM), per kind and
-// storage width from sweeps on the 256^3 porous channel (B200): AA odd and
-// pull are fastest at 8 CTAs/SM (64 registers; FP64 odd 0.963 ms at 6 with
+// storage width from sweeps on the 256^3 porous channel (B200). FP64: AA odd
+// and pull are fastest at 8 CTAs/SM (64 registers; odd 0.963 ms at 6 with
 // the row table in registers, 0.803 at 6 and 0.764 at 8 with it in shared
-// memory); push at 6 for FP64 (0.751 ms; 0.768 at 7, 0.918 at 8), 8 for
-// FP16 (0.364 ms; 0.374 at 7, 0.395 at 6) and 8 for FP32 (0.439 ms; 0.458
-// at 7); the local AA even step (at the HBM limit) does not care.
+// memory), push at 6 (0.751 ms; 0.768 at 7, 0.918 at 8). FP32 and FP16 move
+// a half and a quarter of the bytes and are bound by instruction issue, so
+// more warps in flight pay: AA odd FP32 0.479 / 0.469 / 0.457 / 0.498 ms at
+// 8 / 10 / 12 / 14, FP16 0.437 / 0.430 / 0.410 / 0.404; pull FP32 0.440 /
+// 0.421 / 0.410 / 0.400, FP16 0.382 / 0.363 / 0.367 / 0.368; push stays at
+// 8 (FP32 0.435 ms, FP16 0.362; 10 and 12 are slower). The local AA even
+// step (at the HBM limit) does not care.
 #ifndef LBM_MINB_CP_ODD
 #define LBM_MINB_CP_ODD 8
 #endif
+#ifndef LBM_MINB_CP_ODD_F32
+#define LBM_MINB_CP_ODD_F32 12
+#endif
+#ifndef LBM_MINB_CP_ODD_F16
+#define LBM_MINB_CP_ODD_F16 14
+#endif
 #ifndef LBM_MINB_CP_PULL
 #define LBM_MINB_CP_PULL 8
+#endif
+#ifndef LBM_MINB_CP_PULL_F32
+#define LBM_MINB_CP_PULL_F32 14
+#endif
+#ifndef LBM_MINB_CP_PULL_F16
+#define LBM_MINB_CP_PULL_F16 10
 #endif
 #ifndef LBM_MINB_CP_PUSH_F64
 #define LBM_MINB_CP_PUSH_F64 6
@@ -61,9 +77,12 @@ namespace lbm {
 template <int KIND, int SB> struct CpOccupancy {
   static constexpr int push = SB == 8 ? LBM_MINB_CP_PUSH_F64
       : SB == 4 ? LBM_MINB_CP_PUSH_F32 : LBM_MINB_CP_PUSH_F16;
+  static constexpr int odd = SB == 8 ? LBM_MINB_CP_ODD
+      : SB == 4 ? LBM_MINB_CP_ODD_F32 : LBM_MINB_CP_ODD_F16;
+  static constexpr int pull = SB == 8 ? LBM_MINB_CP_PULL
+      : SB == 4 ? LBM_MINB_CP_PULL_F32 : LBM_MINB_CP_PULL_F16;
   static constexpr int value = KIND == kAAEvenStep ? LBM_MINB_CP_EVEN
-      : KIND == kAAOddStep ? LBM_MINB_CP_ODD
-      : KIND == kPullStep ? LBM_MINB_CP_PULL : push;
+      : KIND == kAAOddStep ? odd : KIND == kPullStep ? pull : push;
 };
 
 // Storage indices of the 18 neighbours of one fluid cell (compact layout).
