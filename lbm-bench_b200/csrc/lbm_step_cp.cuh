@@ -96,6 +96,19 @@ template <int KIND, int SB> struct CpOccupancy {
 #ifndef LBM_CP_SMEM_TAB
 #define LBM_CP_SMEM_TAB 1
 #endif
+// LBM_CP_INNER_ROWS: rows whose 3 x 3 neighbourhood does not wrap (almost
+// all) find their neighbours' index words at fixed strides from their own.
+// Used where it measured faster (256^3 porous channel): AA odd in every
+// precision (FP16 0.404 -> 0.388 ms) and FP16 pull (0.364 -> 0.360); push
+// (FP64 0.751 -> 0.806 ms) and FP32 pull (0.402 -> 0.418) were slower.
+// LBM_CP_GATHER_REGS: the gather takes the table from registers; only the
+// scatter after the collision reads the shared copy.
+#ifndef LBM_CP_INNER_ROWS
+#define LBM_CP_INNER_ROWS 1
+#endif
+#ifndef LBM_CP_GATHER_REGS
+#define LBM_CP_GATHER_REGS 1
+#endif
 constexpr int kTabRows = 13;
 
 template <bool ZPER> struct RowTab {
@@ -109,28 +122,51 @@ template <bool ZPER> struct RowTab {
     return q == 1 ? 9 : q == 3 ? 10 : q == 5 ? 11 : 12;
   }
 
+  __device__ __forceinline__ void row(const Grid &g, int q, uint32_t k, uint32_t lt, int lane)
+  {
+    const uint2 wb = __ldg(g.wb + k);
+    const uint32_t w = wb.x;
+    B[q] = wb.y + (uint32_t)__popc(w & lt);
+    if (q == 1 || q == 3 || q == 5 || q == 7)
+      B[axis_slot(q)] = B[q] + ((w >> lane) & 1u);
+  }
+
+  // k0: index word of the thread's own row, ((x * ny) + y) * W + wi.
+  // INNER: take the stride path for rows away from the box faces.
+  template <bool INNER>
   __device__ __forceinline__ void build(const Grid &g, int x_, int y_, int z_, uint32_t cell,
-      uint32_t wi, uint32_t lt, int lane)
+      uint32_t wi, uint32_t lt, int lane, uint32_t k0)
   {
     x = x_;
     y = y_;
     z = z_;
     B[4] = cell;
+    if (INNER && x > 0 && x < g.nx - 1 && y > 0 && y < g.ny - 1) {
+      // warp-uniform branch: x is the block's plane, y the warp's row
+      const uint32_t sy = (uint32_t)g.W, sx = (uint32_t)g.ny * sy;
 #pragma unroll
-    for (int q = 0; q < 9; ++q) {
-      if (q == 4)
-        continue;
-      int xr = x + q / 3 - 1, yr = y + q % 3 - 1;
-      // out-of-range rows only occur on non-periodic faces, whose cells are
-      // walls (the mask says so and the index is never used): wrap anyway
-      xr = xr < 0 ? g.nx - 1 : xr >= g.nx ? 0 : xr;
-      yr = yr < 0 ? g.ny - 1 : yr >= g.ny ? 0 : yr;
-      const uint32_t k = ((uint32_t)xr * (uint32_t)g.ny + (uint32_t)yr) * (uint32_t)g.W + wi;
-      const uint2 wb = __ldg(g.wb + k);
-      const uint32_t w = wb.x;
-      B[q] = wb.y + (uint32_t)__popc(w & lt);
-      if (q == 1 || q == 3 || q == 5 || q == 7)
-        B[axis_slot(q)] = B[q] + ((w >> lane) & 1u);
+      for (int q = 0; q < 9; ++q) {
+        if (q == 4)
+          continue;
+        const int dx = q / 3 - 1, dy = q % 3 - 1;
+        uint32_t k = k0;
+        k = dx < 0 ? k - sx : dx > 0 ? k + sx : k;
+        k = dy < 0 ? k - sy : dy > 0 ? k + sy : k;
+        row(g, q, k, lt, lane);
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < 9; ++q) {
+        if (q == 4)
+          continue;
+        int xr = x + q / 3 - 1, yr = y + q % 3 - 1;
+        // out-of-range rows only occur on non-periodic faces, whose cells
+        // are walls (the mask says so and the index is never used): wrap
+        xr = xr < 0 ? g.nx - 1 : xr >= g.nx ? 0 : xr;
+        yr = yr < 0 ? g.ny - 1 : yr >= g.ny ? 0 : yr;
+        row(g, q, ((uint32_t)xr * (uint32_t)g.ny + (uint32_t)yr) * (uint32_t)g.W + wi, lt,
+            lane);
+      }
     }
     if (sB) {
 #pragma unroll
@@ -142,13 +178,14 @@ template <bool ZPER> struct RowTab {
       zwrap = z == 0 || z == g.nz - 1;
   }
 
-  __device__ __forceinline__ uint32_t entry(int k) const
+  __device__ __forceinline__ uint32_t entry(int k, bool regs) const
   {
-    return (sB && k != 4) ? sB[k * kStepThreads] : B[k];
+    return (!regs && sB && k != 4) ? sB[k * kStepThreads] : B[k];
   }
 
-  // storage index of x + c_d; meaningful only when that cell is fluid
-  __device__ __forceinline__ uint32_t at(const Grid &g, int d) const
+  // storage index of x + c_d; meaningful only when that cell is fluid.
+  // regs: take the table from registers (while they still hold it)
+  __device__ __forceinline__ uint32_t at(const Grid &g, int d, bool regs = false) const
   {
     const int q = (cx(d) + 1) * 3 + (cy(d) + 1);
     if (ZPER && cz(d) != 0 && zwrap) {
@@ -159,10 +196,10 @@ template <bool ZPER> struct RowTab {
       return packed_index(g, a, b, c);
     }
     if (cz(d) > 0)
-      return q == 4 ? B[4] + 1u : entry(axis_slot(q));
+      return q == 4 ? B[4] + 1u : entry(axis_slot(q), regs);
     if (cz(d) < 0)
-      return entry(q) - 1u;
-    return entry(q);
+      return entry(q, regs) - 1u;
+    return entry(q, regs);
   }
 };
 
@@ -219,8 +256,11 @@ __global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND, sizeof(typena
     __shared__ uint32_t tab[kTabRows * kStepThreads];
     t.sB = tab + (threadIdx.y * blockDim.x + threadIdx.x);
   }
+  constexpr bool kInner = LBM_CP_INNER_ROWS &&
+      (KIND == kAAOddStep || (KIND == kPullStep && sizeof(S) == 2));
   if (KIND != kAAEvenStep)
-    t.build(g, x, y, z, cell, wi, lt, lane);
+    t.template build<kInner>(g, x, y, z, cell, wi, lt, lane, k0);
+  constexpr bool kRegs = LBM_CP_GATHER_REGS != 0;
 
   V f[Q];
   if (KIND == kPushStep || KIND == kAAEvenStep) {
@@ -232,7 +272,8 @@ __global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND, sizeof(typena
     // no lane of the warp has a wall link: no redirects
 #pragma unroll
     for (int d = 0; d < Q; ++d) {
-      const OFF o = (KIND == kPullStep) ? el(d, t.at(g, inv(d))) : el(inv(d), t.at(g, inv(d)));
+      const OFF o = (KIND == kPullStep) ? el(d, t.at(g, inv(d), kRegs))
+                                        : el(inv(d), t.at(g, inv(d), kRegs));
       f[d] = M::ld(a, ldg<kNC>(src + o));
     }
   } else {
@@ -241,9 +282,9 @@ __global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND, sizeof(typena
       const bool back = (mask >> inv(d)) & 1u;
       OFF o;
       if (KIND == kPullStep)
-        o = back ? el(inv(d), cell) : el(d, t.at(g, inv(d)));
+        o = back ? el(inv(d), cell) : el(d, t.at(g, inv(d), kRegs));
       else
-        o = back ? el(d, cell) : el(inv(d), t.at(g, inv(d)));
+        o = back ? el(d, cell) : el(inv(d), t.at(g, inv(d), kRegs));
       f[d] = M::ld(a, ldg<kNC>(src + o));
     }
   }
