@@ -220,6 +220,25 @@ template <class ST> struct CpMathDirect {
   __device__ static V plus(V x, V y) { return x + y; }
 };
 
+// The body-force term of direction d for a cell whose link d is (bb) or is
+// not a wall: force[inv d] or force[d]. Both constants are rounded once from
+// ((3 w_d) c_dx) F, so for c_dx = 0 they are the same value and otherwise
+// force[inv d] is -force[d] bit for bit: the select is a sign flip of one
+// constant, with the same result as loading and selecting two.
+__device__ __forceinline__ float force_term(const float (&force)[Q], int d, bool bb)
+{
+  if (cx(d) == 0)
+    return force[d];
+  return __uint_as_float(__float_as_uint(force[d]) ^ ((uint32_t)bb << 31));
+}
+__device__ __forceinline__ double force_term(const double (&force)[Q], int d, bool bb)
+{
+  if (cx(d) == 0)
+    return force[d];
+  return __longlong_as_double(
+      (long long)((unsigned long long)__double_as_longlong(force[d]) ^ ((unsigned long long)bb << 63)));
+}
+
 // OFF: type of element offsets within the state (uint32_t when all 19
 // planes fit below 2^32 elements, which keeps address arithmetic 32-bit).
 template <class M, int KIND, bool FORCE, bool ZPER, typename OFF>
@@ -295,7 +314,7 @@ __global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND, sizeof(typena
 #pragma unroll
   for (int d = 0; d < Q; ++d) {
     const bool bb = (mask >> d) & 1u;
-    const V v = FORCE ? M::plus(o[d], bb ? a.c.force[inv(d)] : a.c.force[d]) : o[d];
+    const V v = FORCE ? M::plus(o[d], force_term(a.c.force, d, bb)) : o[d];
     OFF off;
     if (KIND == kPullStep)
       off = el(d, cell);
@@ -334,7 +353,7 @@ __global__ void __launch_bounds__(kStepThreads, (CpOccupancy<kAAEvenStep, sizeof
 #pragma unroll
   for (int d = 0; d < Q; ++d) {
     const bool bb = (mask >> d) & 1u;
-    const V v = FORCE ? o[d] + (bb ? a.c.force[inv(d)] : a.c.force[d]) : o[d];
+    const V v = FORCE ? o[d] + force_term(a.c.force, d, bb) : o[d];
     a.dst[inv(d) * P + cell] = ST::encode(v, a.c.scale);
   }
 }
