@@ -11,13 +11,20 @@
 //                           plane is one aligned 8-byte access per thread and
 //                           a warp moves 256 contiguous bytes per plane, with
 //                           no index lookup at all.
-//   pull, push, AA odd      step_kernel_cp (lbm_step_cp.cuh), one cell per
+//   pull, AA odd            step_kernel_cp2_pair below: two cells per thread
+//                           (z and z + 32 of one row) sharing the row's
+//                           index words and every float2 operation. At
+//                           256^3: FP16 AA odd 0.366 against 0.381 ms for one
+//                           cell per thread, FP16 pull 0.329 against 0.359,
+//                           FP32 AA odd 0.429 against 0.455 (64 registers;
+//                           at 6, 7, 9 or 10 CTAs/SM it is slower).
+//   push                    step_kernel_cp (lbm_step_cp.cuh), one cell per
 //                           thread, with CpMathUnits below: the pair
-//                           arithmetic on one cell (collide1). Two cells per
-//                           thread measured slower there (FP16 AA odd 0.61
-//                           against 0.47 ms at 256^3): their accesses are
-//                           per-cell gathers anyway, and the pair halved the
-//                           threads in flight.
+//                           arithmetic on one cell (collide1). The two-cell
+//                           kernel spills there (FP16 push 0.539 against
+//                           0.361 ms). An earlier two-cell form that paired
+//                           consecutive stored cells took 0.61 ms for FP16 AA
+//                           odd: its cells came from different rows.
 #pragma once
 
 #include <type_traits>
@@ -178,5 +185,125 @@ template <class ST> struct CpMathUnits {
   __device__ static void coll(const Args &a, const V (&f)[Q], V (&o)[Q]) { collide1(f, o, a.c); }
   __device__ static V plus(V x, V y) { return __fadd_rn(x, y); }
 };
+
+// Two cells per thread for the non-local kinds (pull, push, AA odd): z and
+// z + 32 of one row, so a warp covers 64 consecutive z and each half of it
+// gathers and scatters exactly as a warp of step_kernel_cp does (32 lanes,
+// coalesced per plane). The two cells share the row's index words, the
+// prologue, the kernel parameters and every float2 operation of collide2 and
+// add_force2 - the dense pair kernels' arithmetic, bit for bit. A solid (or
+// past-the-row) partner is carried with zeros and never loaded or stored.
+// Block (32, 4): four rows of one word pair; grid (ceil(W / 2), ceil(ny / 4),
+// planes).
+#ifndef LBM_MINB_CP2_PAIR
+#define LBM_MINB_CP2_PAIR 8
+#endif
+// Kinds (bit 1 << Kind) that take the two-cell kernel; the others take
+// step_kernel_cp with CpMathUnits. LBM_CP2_PAIR_REGS: its gather takes the
+// row tables from registers (1) or from their shared copies (0).
+#ifndef LBM_CP2_PAIR_KINDS
+#define LBM_CP2_PAIR_KINDS ((1 << kPullStep) | (1 << kAAOddStep))
+#endif
+#ifndef LBM_CP2_PAIR_REGS
+#define LBM_CP2_PAIR_REGS LBM_CP_GATHER_REGS
+#endif
+
+template <class ST, int KIND, bool FORCE, bool ZPER, typename OFF>
+__global__ void __launch_bounds__(kStepThreads, LBM_MINB_CP2_PAIR)
+    step_kernel_cp2_pair(StepArgs2<ST> a)
+{
+  using PT = PairOf<ST>;
+  using S = typename PT::S;
+  constexpr bool kNC = (KIND == kPullStep || KIND == kPushStep);
+  constexpr bool kScatter = (KIND == kPushStep || KIND == kAAOddStep);
+  constexpr bool kInner = LBM_CP_INNER_ROWS &&
+      (KIND == kAAOddStep || (KIND == kPullStep && sizeof(S) == 2));
+  constexpr bool kRegs = LBM_CP2_PAIR_REGS != 0;
+  const Grid &g = a.g;
+  const int lane = threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = a.x0 + (int)blockIdx.z;
+  if (y >= g.ny)
+    return;
+  const uint32_t wi0 = 2u * blockIdx.x; // words wi0 and wi0 + 1 of the row
+  const bool has1 = wi0 + 1u < (uint32_t)g.W;
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t k0 = ((uint32_t)x * (uint32_t)g.ny + (uint32_t)y) * (uint32_t)g.W + wi0;
+  const uint2 wb0 = __ldg(g.wb + k0);
+  const uint2 wb1 = has1 ? __ldg(g.wb + k0 + 1u) : make_uint2(0u, 0u);
+  const bool fl0 = (wb0.x >> lane) & 1u, fl1 = (wb1.x >> lane) & 1u;
+  if (!fl0 && !fl1)
+    return;
+  const uint32_t cell0 = wb0.y + (uint32_t)__popc(wb0.x & lt);
+  const uint32_t cell1 = wb1.y + (uint32_t)__popc(wb1.x & lt);
+  // a cell that is not there has no links: nothing redirects, nothing moves
+  const uint32_t m0 = fl0 ? __ldg(a.mask + cell0) : 0u;
+  const uint32_t m1 = fl1 ? __ldg(a.mask + cell1) : 0u;
+  const S *src = a.src;
+  S *dst = a.dst;
+  const OFF P = (OFF)g.plane;
+  auto el = [&](int plane, uint32_t i) { return (OFF)plane * P + (OFF)i; };
+  auto ld = [&](bool fl, OFF o) { return fl ? PT::dec1(ldg<kNC>(src + o)) : 0.0f; };
+
+  RowTab<ZPER> t0, t1;
+  if (kScatter && LBM_CP_SMEM_TAB) {
+    __shared__ uint32_t tab[2 * kTabRows * kStepThreads];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    t0.sB = tab + tid;
+    t1.sB = tab + kTabRows * kStepThreads + tid;
+  }
+  const int z0 = 32 * (int)wi0 + lane;
+  t0.template build<kInner>(g, x, y, z0, cell0, wi0, lt, lane, k0);
+  if (has1)
+    t1.template build<kInner>(g, x, y, z0 + 32, cell1, wi0 + 1u, lt, lane, k0 + 1u);
+
+  float2 f[Q];
+  if (KIND == kPushStep) {
+#pragma unroll
+    for (int d = 0; d < Q; ++d)
+      f[d] = make_float2(ld(fl0, el(d, cell0)), ld(fl1, el(d, cell1)));
+  } else if (!__any_sync(__activemask(), ((m0 | m1) & 0x7FFFFu) != 0u)) {
+#pragma unroll
+    for (int d = 0; d < Q; ++d) {
+      const int pl = (KIND == kPullStep) ? d : inv(d);
+      f[d] = make_float2(ld(fl0, el(pl, t0.at(g, inv(d), kRegs))),
+                         ld(fl1, el(pl, t1.at(g, inv(d), kRegs))));
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < Q; ++d) {
+      const bool b0 = (m0 >> inv(d)) & 1u, b1 = (m1 >> inv(d)) & 1u;
+      OFF o0, o1;
+      if (KIND == kPullStep) {
+        o0 = b0 ? el(inv(d), cell0) : el(d, t0.at(g, inv(d), kRegs));
+        o1 = b1 ? el(inv(d), cell1) : el(d, t1.at(g, inv(d), kRegs));
+      } else {
+        o0 = b0 ? el(d, cell0) : el(inv(d), t0.at(g, inv(d), kRegs));
+        o1 = b1 ? el(d, cell1) : el(inv(d), t1.at(g, inv(d), kRegs));
+      }
+      f[d] = make_float2(ld(fl0, o0), ld(fl1, o1));
+    }
+  }
+
+  float2 o[Q];
+  collide2<false>(f, o, a.c, make_float2(0.0f, 0.0f), nullptr);
+
+#pragma unroll
+  for (int d = 0; d < Q; ++d) {
+    const float2 v = FORCE ? add_force2(o[d], d, m0, m1, a.c.force) : o[d];
+    OFF off0, off1;
+    if (KIND == kPullStep) {
+      off0 = el(d, cell0);
+      off1 = el(d, cell1);
+    } else {
+      off0 = ((m0 >> d) & 1u) ? el(inv(d), cell0) : el(d, t0.at(g, d));
+      off1 = ((m1 >> d) & 1u) ? el(inv(d), cell1) : el(d, t1.at(g, d));
+    }
+    if (fl0)
+      dst[off0] = PT::enc1(v.x);
+    if (fl1)
+      dst[off1] = PT::enc1(v.y);
+  }
+}
 
 } // namespace lbm

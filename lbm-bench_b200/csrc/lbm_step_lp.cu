@@ -105,11 +105,23 @@ static cudaError_t go_cp2(const StepArgs2<ST> &a, cudaStream_t st)
       step_kernel_cp2_local_ends<ST, FORCE><<<1, 32, 0, st>>>(a);
     return cudaGetLastError();
   } else {
+  const bool zper = (a.g.per & 4) != 0;
+  const bool off32 = (unsigned long long)Q * (unsigned long long)a.g.plane < (1ull << 32);
+  if constexpr (((LBM_CP2_PAIR_KINDS >> KIND) & 1) != 0) {
+    // two cells per thread (z, z + 32): block (32, 4), one word pair per block column
+    const dim3 block(32, 4, 1);
+    const dim3 grid((unsigned)((a.g.W + 1) / 2), (unsigned)((a.g.ny + 3) / 4), (unsigned)a.planes);
+    if (off32)
+      zper ? step_kernel_cp2_pair<ST, KIND, FORCE, true, uint32_t><<<grid, block, 0, st>>>(a)
+           : step_kernel_cp2_pair<ST, KIND, FORCE, false, uint32_t><<<grid, block, 0, st>>>(a);
+    else
+      zper ? step_kernel_cp2_pair<ST, KIND, FORCE, true, uint64_t><<<grid, block, 0, st>>>(a)
+           : step_kernel_cp2_pair<ST, KIND, FORCE, false, uint64_t><<<grid, block, 0, st>>>(a);
+    return cudaGetLastError();
+  }
   dim3 grid, block;
   cell_launch_shape(a.g, grid, block);
   grid.z = a.planes;
-  const bool zper = (a.g.per & 4) != 0;
-  const bool off32 = (unsigned long long)Q * (unsigned long long)a.g.plane < (1ull << 32);
   if (off32)
     zper ? step_kernel_cp<CpMathUnits<ST>, KIND, FORCE, true, uint32_t><<<grid, block, 0, st>>>(a)
          : step_kernel_cp<CpMathUnits<ST>, KIND, FORCE, false, uint32_t><<<grid, block, 0, st>>>(a);
