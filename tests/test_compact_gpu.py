@@ -172,6 +172,36 @@ def test_compact_split_steps_equal_whole_steps(precision):
     assert np.array_equal(states[0][:, m], states[1][:, m])
 
 
+@pytest.mark.parametrize("split", [False, True], ids=["whole", "split"])
+def test_compact_fp16_large_ranges_equal_dense(split):
+    """FP16 AA on 1.3 M stored cells, as whole steps and as split steps whose
+    plane ranges (one plane, 49, 76) start and end anywhere in the storage
+    order and run on two streams: the local even kernel's whole and partial
+    groups and the two-cell odd kernel must give the dense layout's state
+    bit for bit."""
+    flags, _, _ = L.porous_channel((128, 96, 136), 0.2, 3.0, 6.0, seed=12)
+    f0 = L.perturbed_equilibrium(flags, seed=4, amplitude=1e-4)
+    steps = 8
+    d = run(flags, (1, 0, 0), f0, steps, 1.25, 3 / 16, 1e-6, True, "aa", L.F16, compact=False)
+    cuts = [0, 1, 50, 51, 127, 128]
+    with L.Solver(flags, (1, 0, 0), "aa", L.F16, compact=True) as s:
+        assert s.fluid_cells > 1_000_000
+        s.set_params(1.25, 3 / 16, 1e-6, True)
+        s.set_state(f0)
+        for _ in range(steps):
+            if split:
+                s.step_begin()
+                for a, b in zip(cuts[:-1], cuts[1:]):
+                    s.step_planes(a, b, side=(b - a > 1))
+                s.step_end()
+            else:
+                s.run(1)
+        s.synchronize()
+        c = s.get_state()
+    m = O.fluid_mask(flags)
+    assert np.array_equal(c[:, m], d[:, m])
+
+
 def test_compact_reductions_and_transfers_equal_dense():
     flags, _, _ = L.porous_channel((48, 40, 72), 0.25, 3.0, 6.0, seed=5)
     f0 = L.perturbed_equilibrium(flags, seed=9, amplitude=1e-3)
