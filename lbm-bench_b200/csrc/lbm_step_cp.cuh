@@ -109,6 +109,12 @@ template <int KIND, int SB> struct CpOccupancy {
 #ifndef LBM_CP_GATHER_REGS
 #define LBM_CP_GATHER_REGS 1
 #endif
+// LBM_CP_EARLY_ROWS: the neighbour rows' index words and the link mask are
+// loaded together, before the solid lanes leave, instead of the mask first
+// and the rows after the fluid test.
+#ifndef LBM_CP_EARLY_ROWS
+#define LBM_CP_EARLY_ROWS 1
+#endif
 constexpr int kTabRows = 13;
 
 template <bool ZPER> struct RowTab {
@@ -260,10 +266,8 @@ __global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND, sizeof(typena
   const uint32_t k0 = ((uint32_t)x * (uint32_t)g.ny + (uint32_t)y) * (uint32_t)g.W + wi;
   const uint2 wb0 = __ldg(g.wb + k0);
   const uint32_t w0 = wb0.x;
-  if (!((w0 >> lane) & 1u))
-    return;
+  const bool fluid = (w0 >> lane) & 1u;
   const uint32_t cell = wb0.y + (uint32_t)__popc(w0 & lt);
-  const uint32_t mask = __ldg(a.mask + cell);
   const S *src = a.src;
   S *dst = a.dst;
   const OFF P = (OFF)g.plane;
@@ -277,8 +281,22 @@ __global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND, sizeof(typena
   }
   constexpr bool kInner = LBM_CP_INNER_ROWS &&
       (KIND == kAAOddStep || (KIND == kPullStep && sizeof(S) == 2));
-  if (KIND != kAAEvenStep)
+  uint32_t mask;
+  if (LBM_CP_EARLY_ROWS && KIND != kAAEvenStep) {
+    // the mask and the neighbour rows' words in one round trip, before the
+    // solid lanes leave (a solid lane's number may be one past the last
+    // stored cell: it reads word 0 instead)
+    mask = __ldg(a.mask + (fluid ? cell : 0u));
     t.template build<kInner>(g, x, y, z, cell, wi, lt, lane, k0);
+    if (!fluid)
+      return;
+  } else {
+    if (!fluid)
+      return;
+    mask = __ldg(a.mask + cell);
+    if (KIND != kAAEvenStep)
+      t.template build<kInner>(g, x, y, z, cell, wi, lt, lane, k0);
+  }
   constexpr bool kRegs = LBM_CP_GATHER_REGS != 0;
 
   V f[Q];

@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(kStepThreads, LBM_MINB_CP2_PAIR)
   const uint2 wb0 = __ldg(g.wb + k0);
   const uint2 wb1 = has1 ? __ldg(g.wb + k0 + 1u) : make_uint2(0u, 0u);
   const bool fl0 = (wb0.x >> lane) & 1u, fl1 = (wb1.x >> lane) & 1u;
-  if (!fl0 && !fl1)
+  if (!LBM_CP_EARLY_ROWS && !fl0 && !fl1)
     return;
   const uint32_t cell0 = wb0.y + (uint32_t)__popc(wb0.x & lt);
   const uint32_t cell1 = wb1.y + (uint32_t)__popc(wb1.x & lt);
@@ -256,6 +256,8 @@ __global__ void __launch_bounds__(kStepThreads, LBM_MINB_CP2_PAIR)
   t0.template build<kInner>(g, x, y, z0, cell0, wi0, lt, lane, k0);
   if (has1)
     t1.template build<kInner>(g, x, y, z0 + 32, cell1, wi0 + 1u, lt, lane, k0 + 1u);
+  if (LBM_CP_EARLY_ROWS && !fl0 && !fl1) // rows and masks were loaded together
+    return;
 
   float2 f[Q];
   if (KIND == kPushStep) {
