@@ -36,7 +36,8 @@ namespace lbm {
 // storage width from sweeps on the 256^3 porous channel (B200). FP64: AA odd
 // and pull are fastest at 8 CTAs/SM (64 registers; odd 0.963 ms at 6 with
 // the row table in registers, 0.803 at 6 and 0.764 at 8 with it in shared
-// memory), push at 6 (0.751 ms; 0.768 at 7, 0.918 at 8). FP32 and FP16 move
+// memory), push at 7 (0.699 ms; 0.717 at 6, 0.757 at 8, with the row words
+// and mask loaded together). FP32 and FP16 move
 // a half and a quarter of the bytes and are bound by instruction issue, so
 // more warps in flight pay: AA odd FP32 0.479 / 0.469 / 0.457 / 0.498 ms at
 // 8 / 10 / 12 / 14, FP16 0.437 / 0.430 / 0.410 / 0.404; pull FP32 0.440 /
@@ -62,7 +63,7 @@ namespace lbm {
 #define LBM_MINB_CP_PULL_F16 10
 #endif
 #ifndef LBM_MINB_CP_PUSH_F64
-#define LBM_MINB_CP_PUSH_F64 6
+#define LBM_MINB_CP_PUSH_F64 7
 #endif
 #ifndef LBM_MINB_CP_PUSH_F32
 #define LBM_MINB_CP_PUSH_F32 8
