@@ -243,7 +243,11 @@ __global__ void __launch_bounds__(kStepThreads, LBM_MINB_CP2_PAIR)
   S *dst = a.dst;
   const OFF P = (OFF)g.plane;
   auto el = [&](int plane, uint32_t i) { return (OFF)plane * P + (OFF)i; };
-  auto ld = [&](bool fl, OFF o) { return fl ? PT::dec1(ldg<kNC>(src + o)) : 0.0f; };
+  // base + (plane offset + index); (base + index) + plane offset measured
+  // 47% slower (FP16 AA odd 0.537 against 0.364 ms at 256^3)
+  auto gaddr = [&](int plane, uint32_t i) { return src + el(plane, i); };
+  auto saddr = [&](int plane, uint32_t i) { return dst + el(plane, i); };
+  auto ld = [&](bool fl, const S *p) { return fl ? PT::dec1(ldg<kNC>(p)) : 0.0f; };
 
   RowTab<ZPER> t0, t1;
   if (kScatter && LBM_CP_SMEM_TAB) {
@@ -263,27 +267,27 @@ __global__ void __launch_bounds__(kStepThreads, LBM_MINB_CP2_PAIR)
   if (KIND == kPushStep) {
 #pragma unroll
     for (int d = 0; d < Q; ++d)
-      f[d] = make_float2(ld(fl0, el(d, cell0)), ld(fl1, el(d, cell1)));
+      f[d] = make_float2(ld(fl0, gaddr(d, cell0)), ld(fl1, gaddr(d, cell1)));
   } else if (!__any_sync(__activemask(), ((m0 | m1) & 0x7FFFFu) != 0u)) {
 #pragma unroll
     for (int d = 0; d < Q; ++d) {
       const int pl = (KIND == kPullStep) ? d : inv(d);
-      f[d] = make_float2(ld(fl0, el(pl, t0.at(g, inv(d), kRegs))),
-                         ld(fl1, el(pl, t1.at(g, inv(d), kRegs))));
+      f[d] = make_float2(ld(fl0, gaddr(pl, t0.at(g, inv(d), kRegs))),
+                         ld(fl1, gaddr(pl, t1.at(g, inv(d), kRegs))));
     }
   } else {
 #pragma unroll
     for (int d = 0; d < Q; ++d) {
       const bool b0 = (m0 >> inv(d)) & 1u, b1 = (m1 >> inv(d)) & 1u;
-      OFF o0, o1;
+      const S *p0, *p1;
       if (KIND == kPullStep) {
-        o0 = b0 ? el(inv(d), cell0) : el(d, t0.at(g, inv(d), kRegs));
-        o1 = b1 ? el(inv(d), cell1) : el(d, t1.at(g, inv(d), kRegs));
+        p0 = b0 ? gaddr(inv(d), cell0) : gaddr(d, t0.at(g, inv(d), kRegs));
+        p1 = b1 ? gaddr(inv(d), cell1) : gaddr(d, t1.at(g, inv(d), kRegs));
       } else {
-        o0 = b0 ? el(d, cell0) : el(inv(d), t0.at(g, inv(d), kRegs));
-        o1 = b1 ? el(d, cell1) : el(inv(d), t1.at(g, inv(d), kRegs));
+        p0 = b0 ? gaddr(d, cell0) : gaddr(inv(d), t0.at(g, inv(d), kRegs));
+        p1 = b1 ? gaddr(d, cell1) : gaddr(inv(d), t1.at(g, inv(d), kRegs));
       }
-      f[d] = make_float2(ld(fl0, o0), ld(fl1, o1));
+      f[d] = make_float2(ld(fl0, p0), ld(fl1, p1));
     }
   }
 
@@ -293,18 +297,18 @@ __global__ void __launch_bounds__(kStepThreads, LBM_MINB_CP2_PAIR)
 #pragma unroll
   for (int d = 0; d < Q; ++d) {
     const float2 v = FORCE ? add_force2(o[d], d, m0, m1, a.c.force) : o[d];
-    OFF off0, off1;
+    S *q0, *q1;
     if (KIND == kPullStep) {
-      off0 = el(d, cell0);
-      off1 = el(d, cell1);
+      q0 = saddr(d, cell0);
+      q1 = saddr(d, cell1);
     } else {
-      off0 = ((m0 >> d) & 1u) ? el(inv(d), cell0) : el(d, t0.at(g, d));
-      off1 = ((m1 >> d) & 1u) ? el(inv(d), cell1) : el(d, t1.at(g, d));
+      q0 = ((m0 >> d) & 1u) ? saddr(inv(d), cell0) : saddr(d, t0.at(g, d));
+      q1 = ((m1 >> d) & 1u) ? saddr(inv(d), cell1) : saddr(d, t1.at(g, d));
     }
     if (fl0)
-      dst[off0] = PT::enc1(v.x);
+      *q0 = PT::enc1(v.x);
     if (fl1)
-      dst[off1] = PT::enc1(v.y);
+      *q1 = PT::enc1(v.y);
   }
 }
 
