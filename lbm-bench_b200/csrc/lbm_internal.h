@@ -74,4 +74,32 @@ inline void cell_launch_shape(const Grid &g, dim3 &grid, dim3 &block)
   grid = dim3((g.nz + tz - 1) / tz, (g.ny + ty - 1) / ty, g.nx);
 }
 
+// SM count of the current device, looked up once per device (concurrent
+// first calls store the same value); 0 if it cannot be read.
+inline int sm_count()
+{
+  static int cache[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    return 0;
+  if (cache[dev] == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      return 0;
+    cache[dev] = n;
+  }
+  return cache[dev];
+}
+
+// Prefetch distance in x-planes of the compact AA odd step: `tenths` /
+// 10 waves of blocks (a wave: SMs x resident blocks per SM), rounded up to
+// whole planes of `blocks_per_plane`; 0 when tenths is 0.
+inline uint32_t prefetch_planes(int tenths, int blocks_per_sm, unsigned blocks_per_plane)
+{
+  if (tenths <= 0 || blocks_per_plane == 0)
+    return 0;
+  const long long wave = (long long)sm_count() * blocks_per_sm * tenths;
+  return (uint32_t)((wave + 10LL * blocks_per_plane - 1) / (10LL * blocks_per_plane));
+}
+
 } // namespace lbm

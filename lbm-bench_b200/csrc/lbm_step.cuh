@@ -54,6 +54,7 @@ template <class ST> struct StepArgs {
   Consts<V> c;
   int x0 = 0;            // first storage x plane of the launch (grid.z planes from there)
   uint32_t c0 = 0, cn = 0; // compact layout, local steps: storage indices [c0, c0 + cn)
+  uint32_t pf_planes = 0;  // compact AA odd step: L2 prefetch distance in x-planes (0 = none)
 };
 
 // Minimum resident blocks per SM requested from the compiler (caps the

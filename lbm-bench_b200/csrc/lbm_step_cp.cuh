@@ -210,6 +210,69 @@ template <bool ZPER> struct RowTab {
   }
 };
 
+// L2 prefetch of the compact AA odd step in FP64 and FP32 storage
+// (cp_plane_prefetch below), its distance in tenths of a wave of blocks
+// (prefetch_planes(); 0 turns it off). At 256^3 one wave ahead took FP64 AA
+// odd from 0.743 to 0.722 ms and FP32 from 0.434 to 0.401 ms; two and four
+// waves were slower than none. FP16 AA odd (0.365 -> 0.383 ms) and pull
+// (FP64 0.665 -> 0.785 ms, FP16 0.317 -> 0.335 ms) got slower, so those
+// kernels are compiled without it (push was not measured and has none).
+#ifndef LBM_CP_PF_TENTHS
+#define LBM_CP_PF_TENTHS 10
+#endif
+template <int KIND, int SB> constexpr bool cp_prefetches()
+{
+  return LBM_CP_PF_TENTHS > 0 && KIND == kAAOddStep && SB >= 4;
+}
+
+// Asks the L2 for the bytes [lo_b, hi_b) from `base`, widened to 16-byte
+// bounds (cp.async.bulk.prefetch: a hint that returns no data). The caller
+// keeps the widened range inside one allocation.
+__device__ __forceinline__ void l2_prefetch_bytes(const void *base, unsigned long long lo_b,
+    unsigned long long hi_b)
+{
+  lo_b &= ~15ull;
+  hi_b = (hi_b + 15ull) & ~15ull;
+  if (hi_b > lo_b)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                 :: "l"(static_cast<const char *>(base) + lo_b), "r"((uint32_t)(hi_b - lo_b)));
+}
+
+// L2 prefetch of the AA odd step. The stored cells of one x-plane are one
+// contiguous range of every population plane and of the mask array - from
+// the base of the plane's first index word to the end of its last - so the
+// blocks of plane x share out the range of plane x + pf: thread t < 19 of a
+// block asks for the block's slice of population plane t, thread 19 for
+// its slice of the masks. By the time the blocks of plane x + pf run, their
+// own and their neighbours' rows are in the L2. Slices stay inside the
+// range, and the 16-byte widening inside the plane stride (a multiple of
+// 256 bytes) or the mask array (padded to the plane stride).
+template <typename S>
+__device__ __forceinline__ void cp_plane_prefetch(const Grid &g, const S *src,
+    const uint32_t *mask, int x, uint32_t pf)
+{
+  const unsigned t = threadIdx.y * blockDim.x + threadIdx.x;
+  const long long xp = (long long)x + pf;
+  if (t > (unsigned)Q || xp >= g.nx)
+    return;
+  const uint32_t rw = (uint32_t)g.ny * (uint32_t)g.W; // index words per plane
+  const uint32_t kb = (uint32_t)xp * rw;
+  const uint32_t s = __ldg(g.wb + kb).y;
+  const uint2 we = __ldg(g.wb + kb + rw - 1u);
+  const uint32_t e = we.y + (uint32_t)__popc(we.x);
+  const unsigned long long nblk = (unsigned long long)gridDim.x * gridDim.y;
+  const unsigned long long chunk = ((unsigned long long)(e - s) + nblk - 1) / nblk;
+  const unsigned long long cb =
+      s + chunk * ((unsigned long long)blockIdx.y * gridDim.x + blockIdx.x);
+  if (cb >= e)
+    return;
+  const unsigned long long ce = cb + chunk < e ? cb + chunk : e;
+  if (t < (unsigned)Q)
+    l2_prefetch_bytes(src + (long long)t * g.plane, cb * sizeof(S), ce * sizeof(S));
+  else
+    l2_prefetch_bytes(mask, cb * 4ull, ce * 4ull);
+}
+
 // Arithmetic of the compact kernels. CpMathDirect: values as stored and
 // collide() - the FP64 reference arithmetic (bit-identical to LBM-Bench).
 // CpMathUnits (lbm_step_cp2.cuh): FP32/FP16 storage units and the pair
@@ -259,6 +322,8 @@ __global__ void __launch_bounds__(kStepThreads, (CpOccupancy<KIND, sizeof(typena
   const int z = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int x = a.x0 + (int)blockIdx.z;
+  if (cp_prefetches<KIND, sizeof(S)>() && a.pf_planes)
+    cp_plane_prefetch(g, a.src, a.mask, x, a.pf_planes);
   if (z >= g.nz || y >= g.ny)
     return;
   const int lane = z & 31;

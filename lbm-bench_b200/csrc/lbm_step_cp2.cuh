@@ -7,10 +7,10 @@
 // bit-identical states in FP32 and FP16 storage too.
 //
 //   step_kernel_cp2_local   AA even (local): N consecutive stored cells per
-//                           thread (N = 4 for FP16, 2 for FP32), so every
-//                           plane is one aligned 8-byte access per thread and
-//                           a warp moves 256 contiguous bytes per plane, with
-//                           no index lookup at all.
+//                           thread (N = 2; 4 is supported for FP16), so every
+//                           plane is one aligned 4- or 8-byte access per
+//                           thread and a warp moves 128 or 256 contiguous
+//                           bytes per plane, with no index lookup at all.
 //   pull, AA odd            step_kernel_cp2_pair below: two cells per thread
 //                           (z and z + 32 of one row) sharing the row's
 //                           index words and every float2 operation. At
@@ -38,13 +38,17 @@ namespace lbm {
 #ifndef LBM_MINB_CP2_EVEN
 #define LBM_MINB_CP2_EVEN 6
 #endif
+// FP16 local step: two cells per thread at 8 CTAs/SM took 0.193 ms at 256^3
+// against 0.210 ms for four cells per thread at 5 CTAs/SM (96 registers
+// with spills) and 0.211 ms for two cells at 6 CTAs/SM.
 #ifndef LBM_MINB_CP2_EVEN16
-#define LBM_MINB_CP2_EVEN16 5
+#define LBM_MINB_CP2_EVEN16 8
 #endif
 
-// Cells per thread of the local kernel: 8-byte accesses in both storages.
+// Cells per thread of the local kernel in FP16 storage (2 or 4; FP32 takes
+// 2, one 8-byte access per plane).
 #ifndef LBM_CP2_LOCAL16
-#define LBM_CP2_LOCAL16 4
+#define LBM_CP2_LOCAL16 2
 #endif
 template <class ST> struct LocalCells {
   static constexpr int value = sizeof(typename ST::S) == 2 ? LBM_CP2_LOCAL16 : 2;
@@ -223,6 +227,8 @@ __global__ void __launch_bounds__(kStepThreads, LBM_MINB_CP2_PAIR)
   const int lane = threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int x = a.x0 + (int)blockIdx.z;
+  if (cp_prefetches<KIND, sizeof(S)>() && a.pf_planes)
+    cp_plane_prefetch(g, a.src, a.mask, x, a.pf_planes);
   if (y >= g.ny)
     return;
   const uint32_t wi0 = 2u * blockIdx.x; // words wi0 and wi0 + 1 of the row

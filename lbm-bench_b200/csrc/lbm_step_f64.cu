@@ -178,9 +178,10 @@ cudaError_t launch_step_f64(int kind, bool force, bool brink, const StepArgs<Sto
 }
 
 template <class ST, int KIND>
-static cudaError_t go_cp(bool force, const StepArgs<ST> &a, dim3 grid, dim3 block,
+static cudaError_t go_cp(bool force, const StepArgs<ST> &args, dim3 grid, dim3 block,
     cudaStream_t st)
 {
+  StepArgs<ST> a = args;
   if constexpr (KIND == kAAEvenStep) {
     if (a.cn == 0)
       return cudaSuccess;
@@ -191,6 +192,9 @@ static cudaError_t go_cp(bool force, const StepArgs<ST> &a, dim3 grid, dim3 bloc
       step_kernel_cp_local<ST, false><<<nb, kStepThreads, 0, st>>>(a);
     return cudaGetLastError();
   } else {
+  if (cp_prefetches<KIND, sizeof(typename ST::S)>())
+    a.pf_planes = prefetch_planes(LBM_CP_PF_TENTHS,
+        CpOccupancy<KIND, sizeof(typename ST::S)>::value, grid.x * grid.y);
   const bool zper = (a.g.per & 4) != 0;
   const bool off32 = (unsigned long long)Q * (unsigned long long)a.g.plane < (1ull << 32);
   if (off32) {

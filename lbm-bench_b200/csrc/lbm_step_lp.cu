@@ -88,8 +88,9 @@ cudaError_t launch_step_x2_f16(int kind, bool force, bool brink, const StepArgs2
 }
 
 template <class ST, int KIND, bool FORCE>
-static cudaError_t go_cp2(const StepArgs2<ST> &a, cudaStream_t st)
+static cudaError_t go_cp2(const StepArgs2<ST> &args, cudaStream_t st)
 {
+  StepArgs2<ST> a = args;
   if constexpr (KIND == kAAEvenStep) {
     constexpr uint32_t N = LocalCells<ST>::value;
     if (a.cn == 0)
@@ -111,6 +112,8 @@ static cudaError_t go_cp2(const StepArgs2<ST> &a, cudaStream_t st)
     // two cells per thread (z, z + 32): block (32, 4), one word pair per block column
     const dim3 block(32, 4, 1);
     const dim3 grid((unsigned)((a.g.W + 1) / 2), (unsigned)((a.g.ny + 3) / 4), (unsigned)a.planes);
+    if (cp_prefetches<KIND, sizeof(typename ST::S)>())
+      a.pf_planes = prefetch_planes(LBM_CP_PF_TENTHS, LBM_MINB_CP2_PAIR, grid.x * grid.y);
     if (off32)
       zper ? step_kernel_cp2_pair<ST, KIND, FORCE, true, uint32_t><<<grid, block, 0, st>>>(a)
            : step_kernel_cp2_pair<ST, KIND, FORCE, false, uint32_t><<<grid, block, 0, st>>>(a);
