@@ -190,3 +190,54 @@ def test_compact_neighbour_identities():
                     assert idx == rank[xx, yy, zz], (x, y, z, d)
                     checked += 1
     assert checked > 10000
+
+
+def _prefetch_slices(bits, base, nx, ny, W, nblk, xp):
+    """The slices of plane xp that the nblk blocks of one plane ask the L2
+    for in the compact AA odd step (cp_plane_prefetch, lbm_step_cp.cuh):
+    [s, e) from the base of the plane's first index word to the end of its
+    last, split in ceil((e - s) / nblk) cells per block."""
+    kb = xp * ny * W
+    s = int(base.reshape(-1)[kb])
+    ke = kb + ny * W - 1
+    e = int(base.reshape(-1)[ke]) + bin(int(bits.reshape(-1)[ke])).count("1")
+    chunk = (e - s + nblk - 1) // nblk
+    out = []
+    for part in range(nblk):
+        cb = s + chunk * part
+        if cb < e:
+            out.append((cb, min(cb + chunk, e)))
+    return s, e, out
+
+
+@pytest.mark.parametrize("dims,nblk", [((24, 20, 70), 20), ((16, 9, 36), 9), ((12, 8, 200), 16),
+                                       ((10, 6, 33), 200)])
+def test_compact_prefetch_slices_stay_in_bounds(dims, nblk):
+    """The L2 prefetch of the compact AA odd step widens each block's slice
+    to 16-byte bounds. For every plane the slices must tile exactly the
+    plane's stored cells, and the widened byte ranges must stay inside one
+    population plane (stride rounded up to 256 bytes) and inside the mask
+    array (padded to the same stride), in FP64, FP32 and FP16 storage."""
+    nx, ny, nz = dims
+    rng = np.random.default_rng(nx * ny + nz)
+    fluid = rng.uniform(size=(nx, ny, nz)) > 0.25
+    bits, base, total = L.compact_index(fluid.reshape(nx * ny, nz), nz)
+    W = bits.shape[1]
+    starts = []
+    for xp in range(nx):
+        s, e, sl = _prefetch_slices(bits, base, nx, ny, W, nblk, xp)
+        assert e - s == int(fluid[xp].sum())
+        starts.append(s)
+        covered = 0
+        for cb, ce in sl:
+            assert s <= cb < ce <= e
+            covered += ce - cb
+        assert covered == e - s
+        for size in (8, 4, 2):
+            plane = (total + 256 // size - 1) // (256 // size) * (256 // size)
+            for cb, ce in sl:
+                lo, hi = (cb * size) & ~15, (ce * size + 15) & ~15
+                assert 0 <= lo < hi <= plane * size
+                lo4, hi4 = (cb * 4) & ~15, (ce * 4 + 15) & ~15
+                assert 0 <= lo4 < hi4 <= plane * 4
+    assert starts == sorted(starts)
